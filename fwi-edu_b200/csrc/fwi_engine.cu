@@ -1,0 +1,1093 @@
+// fwi_engine.cu -- host side of the B200 engine and its C-ABI.
+//
+// A context (fwi_ctx) holds one model on the global grid, the shots, and every
+// device buffer a run needs.  Shots that share a model window and wavelet peak
+// frequency share one Plan (the coefficient fields of propagation.c:508-532),
+// uploaded once per model version.  Each shot owns its wavefield storage:
+// checkpoint frames, scratch frames, the replayed frames kept for imaging, FP64
+// accumulators and its gathers.
+//
+// A run is a sequence of launches of k_step.  What each launch does for each
+// shot is read from a small program on the device (int4 per launch: up to two
+// items, e.g. a replay step of one segment next to an adjoint step of another),
+// so the host loop only issues launches.  On the batched path all shots of a
+// group go into every launch and the whole launch sequence is captured once as
+// a CUDA graph and replayed; on the plain path shots run one after another, one
+// launch per step, as the reference's shot loop does (propagation.c:857, :895).
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdarg>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <deque>
+#include <map>
+#include <memory>
+#include <string>
+#include <vector>
+
+#include "../../include/fwi_b200.h"
+#include "fwi_aux.cuh"
+#include "fwi_kernels.cuh"
+#include "fwi_setup.h"
+
+using namespace fwi;
+
+// ---------------------------------------------------------------- errors
+static thread_local std::string g_err;
+static int fail(int code, const char *fmt, ...)
+{
+    char buf[1024];
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(buf, sizeof(buf), fmt, ap);
+    va_end(ap);
+    g_err = buf;
+    return code;
+}
+#define CK(call)                                                                                       \
+    do {                                                                                               \
+        cudaError_t e_ = (call);                                                                       \
+        if (e_ != cudaSuccess) return fail(FWI_ERR_CUDA, "%s failed: %s", #call, cudaGetErrorString(e_)); \
+    } while (0)
+#define TRY(call)                 \
+    do {                          \
+        int r_ = (call);          \
+        if (r_ != FWI_OK) return r_; \
+    } while (0)
+
+extern "C" const char *fwi_last_error(void) { return g_err.c_str(); }
+extern "C" const char *fwi_version(void) { return "fwi-b200 0.1 (sm_100a)"; }
+
+// ---------------------------------------------------------------- context
+struct ShotHost {
+    fwi_shot s;
+    std::vector<float> src;
+    std::vector<int> igx, igz;
+};
+
+struct Plan {
+    int ix_min = 0, ix_max = -1;
+    float fpeak = 0.f;
+    unsigned long long version = ~0ull;
+    fwi_coefs hc{};
+    float *d_coef = nullptr;  // c1, c2, ck, irx, irz, ir, each Nx*ld
+    int Nx = 0, Nz = 0, ld = 0, G = 0;
+    size_t frame() const { return (size_t)Nx * ld; }
+};
+
+struct ShotRun {
+    int shot = -1;
+    Plan *plan = nullptr;
+    ShotDesc d{};
+    // per-run host-side extras
+    int Lt = 0, Lr = 0;
+    float *d_tct = nullptr, *d_tcr = nullptr;
+    float *d_gshot = nullptr, *d_hshot = nullptr;  // [nxx][nz] FP32 per-shot gradient / preconditioner
+    bool has_ck = false;
+    std::vector<void *> allocs;
+};
+
+struct Program {
+    std::vector<int4> items;
+    int4 *d = nullptr;
+};
+
+struct fwi_ctx {
+    int device = 0;
+    size_t budget = 0, used = 0;
+    cudaStream_t stream = nullptr;
+    cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+    // model and run constants
+    int nz = 0, nx = 0, nt = 0, pml = 0, fs = 0;
+    float dx = 0, dz = 0, dt = 0;
+    std::vector<float> vp, rho;
+    float *d_vp = nullptr, *d_rho = nullptr;
+    unsigned long long version = 0;
+    bool host_model_valid = false;
+    // shots
+    std::vector<ShotHost> shots;
+    std::vector<float *> d_obs, d_pre;
+    std::vector<std::unique_ptr<Plan>> plans;
+    std::vector<std::unique_ptr<ShotRun>> runs;  // one per shot (batched) or one reused (plain)
+    ShotDesc *d_desc = nullptr;
+    int desc_cap = 0;
+    // survey-wide outputs
+    float *d_grad = nullptr, *d_prec = nullptr;
+    double *d_gc = nullptr, *d_hc = nullptr;
+    double *d_red = nullptr;     // reduction partials + results
+    void *d_scratch = nullptr;   // small descriptor arrays
+    size_t scratch_cap = 0;
+    // programs and graphs, keyed by (kind, overlap)
+    std::map<std::string, Program> progs;
+    std::map<std::string, cudaGraphExec_t> graphs;
+    fwi_stats stats{};
+    long long launches = 0;
+    double last_obj = 0.0;
+};
+
+static int dmalloc(fwi_ctx *c, void **p, size_t bytes)
+{
+    if (c->budget && c->used + bytes > c->budget)
+        return fail(FWI_ERR_NOMEM, "device budget exceeded: %zu + %zu > %zu bytes", c->used, bytes, c->budget);
+    cudaError_t e = cudaMalloc(p, bytes ? bytes : 16);
+    if (e != cudaSuccess) return fail(FWI_ERR_NOMEM, "cudaMalloc(%zu): %s", bytes, cudaGetErrorString(e));
+    c->used += bytes;
+    return FWI_OK;
+}
+static void dfree(fwi_ctx *c, void *p, size_t bytes)
+{
+    if (p) {
+        cudaFree(p);
+        c->used -= std::min(c->used, bytes);
+    }
+}
+
+static void free_run(fwi_ctx *c, ShotRun *r)
+{
+    for (void *p : r->allocs) cudaFree(p);
+    r->allocs.clear();
+    (void)c;
+}
+
+static void drop_graphs(fwi_ctx *c)
+{
+    for (auto &kv : c->graphs) cudaGraphExecDestroy(kv.second);
+    c->graphs.clear();
+}
+
+static void free_runs(fwi_ctx *c)
+{
+    drop_graphs(c);
+    for (auto &r : c->runs) free_run(c, r.get());
+    c->runs.clear();
+}
+
+extern "C" int fwi_ctx_create(fwi_ctx **out, int device, size_t budget)
+{
+    if (!out) return fail(FWI_ERR_ARG, "ctx pointer is NULL");
+    int n = 0;
+    if (cudaGetDeviceCount(&n) != cudaSuccess || n == 0)
+        return fail(FWI_ERR_NODEVICE, "no CUDA device: this engine runs on the GPU only");
+    if (device < 0 || device >= n) return fail(FWI_ERR_ARG, "device %d out of range (%d devices)", device, n);
+    CK(cudaSetDevice(device));
+    fwi_ctx *c = new fwi_ctx();
+    c->device = device;
+    c->budget = budget;
+    CK(cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking));
+    CK(cudaEventCreate(&c->ev0));
+    CK(cudaEventCreate(&c->ev1));
+    *out = c;
+    return FWI_OK;
+}
+
+extern "C" int fwi_ctx_destroy(fwi_ctx *c)
+{
+    if (!c) return FWI_OK;
+    cudaSetDevice(c->device);
+    cudaStreamSynchronize(c->stream);
+    free_runs(c);
+    for (auto &kv : c->progs) cudaFree(kv.second.d);
+    for (auto &p : c->plans) {
+        cudaFree(p->d_coef);
+        fwi_free_coefs(&p->hc);
+    }
+    for (float *p : c->d_obs) cudaFree(p);
+    for (float *p : c->d_pre) cudaFree(p);
+    cudaFree(c->d_vp); cudaFree(c->d_rho); cudaFree(c->d_grad); cudaFree(c->d_prec);
+    cudaFree(c->d_gc); cudaFree(c->d_hc); cudaFree(c->d_red); cudaFree(c->d_scratch); cudaFree(c->d_desc);
+    cudaEventDestroy(c->ev0); cudaEventDestroy(c->ev1);
+    cudaStreamDestroy(c->stream);
+    delete c;
+    return FWI_OK;
+}
+
+// ---------------------------------------------------------------- model / shots
+static int set_model_common(fwi_ctx *c, int nz, int nx, float dx, float dz, float dt, int nt, int pml, int fs)
+{
+    if (nz <= 0 || nx <= 0 || nt <= 0 || pml < 0 || !(dx > 0) || !(dz > 0) || !(dt > 0))
+        return fail(FWI_ERR_ARG, "invalid grid: nz=%d nx=%d nt=%d pml=%d dx=%g dz=%g dt=%g", nz, nx, nt, pml, dx, dz, dt);
+    if (fs && pml < 3) return fail(FWI_ERR_ARG, "a free surface needs pmlThick >= 3 (got %d)", pml);
+    bool same = nz == c->nz && nx == c->nx && nt == c->nt && pml == c->pml && fs == c->fs && dx == c->dx &&
+                dz == c->dz && dt == c->dt;
+    if (!same) {
+        free_runs(c);
+        for (auto &kv : c->progs) cudaFree(kv.second.d);
+        c->progs.clear();
+        for (auto &p : c->plans) {
+            cudaFree(p->d_coef);
+            fwi_free_coefs(&p->hc);
+        }
+        c->plans.clear();
+        dfree(c, c->d_vp, 0); dfree(c, c->d_rho, 0);
+        dfree(c, c->d_grad, 0); dfree(c, c->d_prec, 0); dfree(c, c->d_gc, 0); dfree(c, c->d_hc, 0);
+        c->d_vp = c->d_rho = c->d_grad = c->d_prec = nullptr;
+        c->d_gc = c->d_hc = nullptr;
+        size_t m = (size_t)nz * nx;
+        TRY(dmalloc(c, (void **)&c->d_vp, m * 4));
+        TRY(dmalloc(c, (void **)&c->d_rho, m * 4));
+        TRY(dmalloc(c, (void **)&c->d_grad, m * 4));
+        TRY(dmalloc(c, (void **)&c->d_prec, m * 4));
+        TRY(dmalloc(c, (void **)&c->d_gc, m * 8));
+        TRY(dmalloc(c, (void **)&c->d_hc, m * 8));
+    }
+    c->nz = nz; c->nx = nx; c->nt = nt; c->pml = pml; c->fs = fs;
+    c->dx = dx; c->dz = dz; c->dt = dt;
+    c->version++;
+    return FWI_OK;
+}
+
+extern "C" int fwi_ctx_set_model(fwi_ctx *c, const float *vp, const float *rho, int nz, int nx, float dx, float dz,
+                                 float dt, int nt, int pml, int fs)
+{
+    if (!c || !vp || !rho) return fail(FWI_ERR_ARG, "NULL argument to fwi_ctx_set_model");
+    CK(cudaSetDevice(c->device));
+    TRY(set_model_common(c, nz, nx, dx, dz, dt, nt, pml, fs));
+    size_t m = (size_t)nz * nx;
+    for (size_t i = 0; i < m; i++)
+        if (!(vp[i] > 0.0f) || !(rho[i] > 0.0f)) return fail(FWI_ERR_ARG, "vp and rho must be positive (cell %zu)", i);
+    c->vp.assign(vp, vp + m);
+    c->rho.assign(rho, rho + m);
+    c->host_model_valid = true;
+    CK(cudaMemcpyAsync(c->d_vp, vp, m * 4, cudaMemcpyHostToDevice, c->stream));
+    CK(cudaMemcpyAsync(c->d_rho, rho, m * 4, cudaMemcpyHostToDevice, c->stream));
+    return FWI_OK;
+}
+
+extern "C" int fwi_ctx_set_model_device(fwi_ctx *c, const float *d_vp, const float *d_rho, int nz, int nx, float dx,
+                                        float dz, float dt, int nt, int pml, int fs)
+{
+    if (!c || !d_vp || !d_rho) return fail(FWI_ERR_ARG, "NULL argument to fwi_ctx_set_model_device");
+    CK(cudaSetDevice(c->device));
+    TRY(set_model_common(c, nz, nx, dx, dz, dt, nt, pml, fs));
+    size_t m = (size_t)nz * nx;
+    CK(cudaMemcpyAsync(c->d_vp, d_vp, m * 4, cudaMemcpyDeviceToDevice, c->stream));
+    CK(cudaMemcpyAsync(c->d_rho, d_rho, m * 4, cudaMemcpyDeviceToDevice, c->stream));
+    // the coefficient set-up runs on the host with the C library's libm: bring the model over
+    c->vp.resize(m);
+    c->rho.resize(m);
+    CK(cudaMemcpyAsync(c->vp.data(), c->d_vp, m * 4, cudaMemcpyDeviceToHost, c->stream));
+    CK(cudaMemcpyAsync(c->rho.data(), c->d_rho, m * 4, cudaMemcpyDeviceToHost, c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+    c->host_model_valid = true;
+    return FWI_OK;
+}
+
+static bool in_fd_range(int x, int z, int nz, int nxx, int pml, int fs)
+{
+    int X = x + pml, Z = z + pml, Nx = nxx + 2 * pml, Nz = nz + 2 * pml;
+    int z0 = fs ? pml : 3;
+    return x >= 0 && x < nxx && z >= 0 && z < nz && X >= 3 && X <= Nx - 4 && Z >= z0 && Z <= Nz - 4;
+}
+
+extern "C" int fwi_ctx_set_shots(fwi_ctx *c, const fwi_shot *shots, int nshot)
+{
+    if (!c || (!shots && nshot > 0) || nshot < 0) return fail(FWI_ERR_ARG, "invalid shots");
+    if (c->nz <= 0) return fail(FWI_ERR_STATE, "set the model before the shots");
+    CK(cudaSetDevice(c->device));
+    for (int i = 0; i < nshot; i++) {
+        const fwi_shot &s = shots[i];
+        int nxx = s.ix_max - s.ix_min + 1;
+        if (s.ix_min < 0 || s.ix_max >= c->nx || nxx <= 0) return fail(FWI_ERR_ARG, "shot %d: bad window [%d,%d]", i, s.ix_min, s.ix_max);
+        if (s.ntr <= 0 || s.ns <= 0 || s.sampleRate <= 0 || !s.src || !s.igx || !s.igz)
+            return fail(FWI_ERR_ARG, "shot %d: ntr=%d ns=%d sampleRate=%d", i, s.ntr, s.ns, s.sampleRate);
+        if ((c->nt - 1) / s.sampleRate + 1 > s.ns) return fail(FWI_ERR_ARG, "shot %d: ns=%d too short for nt=%d", i, s.ns, c->nt);
+        if (!in_fd_range(s.isx, s.isz, c->nz, nxx, c->pml, c->fs))
+            return fail(FWI_ERR_ARG, "shot %d: source (%d,%d) outside the updated grid", i, s.isx, s.isz);
+        for (int r = 0; r < s.ntr; r++)
+            if (!in_fd_range(s.igx[r], s.igz[r], c->nz, nxx, c->pml, c->fs))
+                return fail(FWI_ERR_ARG, "shot %d: receiver %d (%d,%d) outside the updated grid", i, r, s.igx[r], s.igz[r]);
+    }
+    free_runs(c);
+    for (float *p : c->d_obs) dfree(c, p, 0);
+    for (float *p : c->d_pre) dfree(c, p, 0);
+    c->d_obs.clear();
+    c->d_pre.clear();
+    c->shots.clear();
+    for (int i = 0; i < nshot; i++) {
+        ShotHost h;
+        h.s = shots[i];
+        h.src.assign(shots[i].src, shots[i].src + c->nt);
+        h.igx.assign(shots[i].igx, shots[i].igx + shots[i].ntr);
+        h.igz.assign(shots[i].igz, shots[i].igz + shots[i].ntr);
+        h.s.src = h.src.data();
+        h.s.igx = h.igx.data();
+        h.s.igz = h.igz.data();
+        c->shots.push_back(std::move(h));
+        float *o = nullptr, *p = nullptr;
+        size_t nb = (size_t)shots[i].ntr * shots[i].ns * 4;
+        TRY(dmalloc(c, (void **)&o, nb));
+        TRY(dmalloc(c, (void **)&p, nb));
+        CK(cudaMemsetAsync(o, 0, nb, c->stream));
+        CK(cudaMemsetAsync(p, 0, nb, c->stream));
+        c->d_obs.push_back(o);
+        c->d_pre.push_back(p);
+    }
+    return FWI_OK;
+}
+
+extern "C" int fwi_ctx_set_observed(fwi_ctx *c, const float *const *obs)
+{
+    if (!c || !obs) return fail(FWI_ERR_ARG, "NULL argument");
+    CK(cudaSetDevice(c->device));
+    for (size_t i = 0; i < c->shots.size(); i++) {
+        if (!obs[i]) return fail(FWI_ERR_ARG, "observed gather %zu is NULL", i);
+        CK(cudaMemcpyAsync(c->d_obs[i], obs[i], (size_t)c->shots[i].s.ntr * c->shots[i].s.ns * 4,
+                           cudaMemcpyHostToDevice, c->stream));
+    }
+    return FWI_OK;
+}
+
+// ---------------------------------------------------------------- plans
+static int get_plan(fwi_ctx *c, const fwi_shot &s, Plan **out)
+{
+    Plan *p = nullptr;
+    for (auto &q : c->plans)
+        if (q->ix_min == s.ix_min && q->ix_max == s.ix_max && q->fpeak == s.fpeak) p = q.get();
+    if (!p) {
+        c->plans.emplace_back(new Plan());
+        p = c->plans.back().get();
+        p->ix_min = s.ix_min;
+        p->ix_max = s.ix_max;
+        p->fpeak = s.fpeak;
+    }
+    if (p->version != c->version) {
+        if (!c->host_model_valid) return fail(FWI_ERR_STATE, "model not set");
+        int nxx = s.ix_max - s.ix_min + 1;
+        fwi_coefs nc;
+        if (fwi_setup_coefs(c->vp.data() + (size_t)s.ix_min * c->nz, c->rho.data() + (size_t)s.ix_min * c->nz, c->nz,
+                            nxx, c->pml, c->dx, c->dz, c->dt, s.fpeak, &nc))
+            return fail(FWI_ERR_NOMEM, "host allocation failed in the coefficient set-up");
+        size_t fr = (size_t)nc.Nx * nc.ld;
+        if (!p->d_coef || p->Nx != nc.Nx || p->ld != nc.ld) {
+            dfree(c, p->d_coef, 0);
+            p->d_coef = nullptr;
+            TRY(dmalloc(c, (void **)&p->d_coef, 6 * fr * 4));
+        }
+        fwi_free_coefs(&p->hc);
+        p->hc = nc;
+        p->Nx = nc.Nx; p->Nz = nc.Nz; p->ld = nc.ld; p->G = nc.ld / 4;
+        const float *src[6] = {nc.c1, nc.c2, nc.ck, nc.irx, nc.irz, nc.ir};
+        for (int k = 0; k < 6; k++)
+            CK(cudaMemcpyAsync(p->d_coef + k * fr, src[k], fr * 4, cudaMemcpyHostToDevice, c->stream));
+        // the host copy must outlive the asynchronous upload
+        CK(cudaStreamSynchronize(c->stream));
+        p->version = c->version;
+    }
+    *out = p;
+    return FWI_OK;
+}
+
+// ---------------------------------------------------------------- per-shot state
+static int ralloc(fwi_ctx *c, ShotRun *r, void **p, size_t bytes)
+{
+    TRY(dmalloc(c, p, bytes));
+    r->allocs.push_back(*p);
+    return FWI_OK;
+}
+
+// fill the geometry/coefficients part of a descriptor; allocate what the run needs
+static int prepare_run(fwi_ctx *c, ShotRun *r, int shot, bool gradient)
+{
+    const ShotHost &sh = c->shots[shot];
+    const fwi_shot &s = sh.s;
+    Plan *p = nullptr;
+    TRY(get_plan(c, s, &p));
+    const bool same_geom = r->plan && r->plan->Nx == p->Nx && r->plan->ld == p->ld && r->shot >= 0 &&
+                           c->shots[r->shot].s.ntr == s.ntr && c->shots[r->shot].s.ns == s.ns;
+    const bool realloc = !same_geom || (gradient && !r->has_ck) || r->allocs.empty();
+    if (realloc) {
+        free_run(c, r);
+        r->has_ck = false;
+    }
+    r->shot = shot;
+    r->plan = p;
+    ShotDesc &d = r->d;
+    const fwi_coefs &hc = p->hc;
+    d.Nx = p->Nx; d.Nz = p->Nz; d.ld = p->ld; d.G = p->G; d.pml = c->pml;
+    d.nz = c->nz; d.nxx = s.ix_max - s.ix_min + 1; d.fs = c->fs; d.izStart = c->fs ? c->pml : 3;
+    d.nt = c->nt; d.d = fwi_ck_interval(c->nt); d.K = (c->nt - 1) / d.d;
+    d.ns = s.ns; d.sr = s.sampleRate; d.ntr = s.ntr;
+    d.S5 = d.d / MST + 2;
+    d.isx = s.isx + c->pml; d.isz = s.isz + c->pml;
+    d.invdx = hc.invdx; d.invdz = hc.invdz; d.invdxdx = hc.invdxdx; d.invdzdz = hc.invdzdz;
+    d.invdtdt = hc.invdtdt; d.dt = c->dt;
+    const size_t fr = p->frame();
+    d.frame = (long long)fr;
+    d.c1 = p->d_coef; d.c2 = p->d_coef + fr; d.ck = p->d_coef + 2 * fr;
+    d.irx = p->d_coef + 3 * fr; d.irz = p->d_coef + 4 * fr; d.ir = p->d_coef + 5 * fr;
+    const int nt = c->nt, ntr = s.ntr;
+    if (realloc) {
+        void *q;
+        TRY(ralloc(c, r, &q, (size_t)nt * 8)); d.srcd = (double *)q;
+        TRY(ralloc(c, r, &q, (size_t)nt * 4)); d.srcf = (float *)q;
+        TRY(ralloc(c, r, &q, (size_t)(d.Nx + 1) * 4)); d.colptr = (int *)q;
+        TRY(ralloc(c, r, &q, (size_t)ntr * 8)); d.rec = (int2 *)q;
+        TRY(ralloc(c, r, &q, (size_t)ntr * 4)); d.recK = (float *)q;
+        TRY(ralloc(c, r, &q, (size_t)s.ns * ntr * 4)); d.traces_t = (float *)q;
+        TRY(ralloc(c, r, &q, 3 * fr * 4)); d.fscr = (float *)q;
+        d.ckslots = d.rscr = d.seg = d.ascr = nullptr;
+        d.H = d.Gacc = nullptr;
+        d.adj_t = nullptr;
+        if (gradient) {
+            TRY(ralloc(c, r, &q, (size_t)(2 * (d.K + 1)) * fr * 4)); d.ckslots = (float *)q;
+            TRY(ralloc(c, r, &q, 3 * fr * 4)); d.rscr = (float *)q;
+            TRY(ralloc(c, r, &q, (size_t)(2 * d.S5) * fr * 4)); d.seg = (float *)q;
+            TRY(ralloc(c, r, &q, 3 * fr * 4)); d.ascr = (float *)q;
+            TRY(ralloc(c, r, &q, fr * 8)); d.H = (double *)q;
+            TRY(ralloc(c, r, &q, fr * 8)); d.Gacc = (double *)q;
+            TRY(ralloc(c, r, &q, (size_t)nt * ntr * 4)); d.adj_t = (float *)q;
+            size_t m = (size_t)c->nz * d.nxx;
+            TRY(ralloc(c, r, &q, m * 4)); r->d_gshot = (float *)q;
+            TRY(ralloc(c, r, &q, m * 4)); r->d_hshot = (float *)q;
+            TRY(ralloc(c, r, &q, (size_t)(s.ns + 1) * 4)); r->d_tct = (float *)q;
+            TRY(ralloc(c, r, &q, (size_t)(ntr + 1) * 4)); r->d_tcr = (float *)q;
+            r->has_ck = true;
+        } else {
+            void *q2;
+            TRY(ralloc(c, r, &q2, (size_t)(s.ns + 1) * 4)); r->d_tct = (float *)q2;
+            TRY(ralloc(c, r, &q2, (size_t)(ntr + 1) * 4)); r->d_tcr = (float *)q2;
+        }
+    }
+    d.hessian = 0;
+    // per-step source terms in the reference's precision (propagation.c:558 double, :662 float)
+    const float Ks = hc.K[(size_t)d.isx * d.ld + d.isz];
+    std::vector<double> sd(nt);
+    std::vector<float> sf(nt);
+    for (int it = 0; it < nt; it++) {
+        sd[it] = fwi_src_term_f64(sh.src[it], Ks, c->dt, hc.invdx, hc.invdz);
+        sf[it] = fwi_src_term_f32(sh.src[it], Ks, c->dt, hc.invdx, hc.invdz);
+    }
+    // receivers as per-column lists sorted by (x, z, trace): duplicates stay in trace order
+    std::vector<int> order(ntr);
+    for (int i = 0; i < ntr; i++) order[i] = i;
+    std::stable_sort(order.begin(), order.end(), [&](int a, int b) {
+        if (sh.igx[a] != sh.igx[b]) return sh.igx[a] < sh.igx[b];
+        return sh.igz[a] < sh.igz[b];
+    });
+    std::vector<int> colptr(d.Nx + 1, 0);
+    std::vector<int2> rec(ntr);
+    std::vector<float> recK(ntr);
+    for (int e = 0; e < ntr; e++) {
+        int i = order[e];
+        int X = sh.igx[i] + c->pml, Z = sh.igz[i] + c->pml;
+        rec[e] = make_int2(Z, i);
+        recK[e] = hc.K[(size_t)X * d.ld + Z];
+        colptr[X + 1]++;
+    }
+    for (int x = 0; x < d.Nx; x++) colptr[x + 1] += colptr[x];
+    CK(cudaMemcpyAsync((void *)d.srcd, sd.data(), nt * 8, cudaMemcpyHostToDevice, c->stream));
+    CK(cudaMemcpyAsync((void *)d.srcf, sf.data(), nt * 4, cudaMemcpyHostToDevice, c->stream));
+    CK(cudaMemcpyAsync((void *)d.colptr, colptr.data(), (d.Nx + 1) * 4, cudaMemcpyHostToDevice, c->stream));
+    CK(cudaMemcpyAsync((void *)d.rec, rec.data(), ntr * 8, cudaMemcpyHostToDevice, c->stream));
+    CK(cudaMemcpyAsync((void *)d.recK, recK.data(), ntr * 4, cudaMemcpyHostToDevice, c->stream));
+    CK(cudaStreamSynchronize(c->stream));  // host staging vectors go out of scope
+    return FWI_OK;
+}
+
+// taper lengths of compute_adjoint_source2d (optimization.c:347-365) and the taper_traces caps
+static int prepare_taper(fwi_ctx *c, ShotRun *r, float freq)
+{
+    const fwi_shot &s = c->shots[r->shot].s;
+    double vp_sum = 0.0;
+    for (int i = 0; i < s.ntr; i++)  // window-local igx into the global model, as the reference does
+        vp_sum += c->vp[(size_t)s.igx[i] * c->nz + s.igz[i]];
+    float vp_avg = (float)(vp_sum / s.ntr);
+    if (freq == 0.0f) freq = s.fpeak;
+    float kpass = freq / vp_avg;
+    int Lt = (int)roundf((2.0f / freq) / s.dt) + 1;
+    int Lr = (int)roundf((2.0f / kpass) / s.dtr) + 1;
+    if (Lt > 0 && Lt > s.ns / 3) Lt = s.ns / 3;
+    if (Lr > 0 && Lr > s.ntr / 3) Lr = s.ntr / 3;
+    if (Lt < 0) Lt = 0;
+    if (Lr < 0) Lr = 0;
+    r->Lt = Lt;
+    r->Lr = Lr;
+    std::vector<float> a(Lt + 1), b(Lr + 1);
+    if (Lt > 0) fwi_taper_coefs(Lt, a.data());
+    if (Lr > 0) fwi_taper_coefs(Lr, b.data());
+    CK(cudaMemcpyAsync(r->d_tct, a.data(), (Lt + 1) * 4, cudaMemcpyHostToDevice, c->stream));
+    CK(cudaMemcpyAsync(r->d_tcr, b.data(), (Lr + 1) * 4, cudaMemcpyHostToDevice, c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+    return FWI_OK;
+}
+
+// ---------------------------------------------------------------- programs
+static bool is_stored(int t, int nt, int d) { return t % d == 0 || ((t + 1) % d == 0 && t + 1 < nt); }
+
+static std::vector<int4> program_forward(int nt, int kind)
+{
+    std::vector<int4> p(nt);
+    for (int it = 0; it < nt; it++) p[it] = make_int4(kind, it, K_NONE, 0);
+    return p;
+}
+
+// adjoint pass: replay segments and adjoint steps.  Without overlap this is the
+// reference's order (replay a whole segment when the reverse loop reaches its top,
+// propagation.c:641-673).  With overlap the replay of segment k-1 runs in the same
+// launches as the adjoint steps of segment k; segments alternate between two frame
+// buffers, so segment k may start once the adjoint no longer needs segment k+2.
+static std::vector<int4> program_adjoint(int nt, bool overlap)
+{
+    const int d = fwi_ck_interval(nt), K = (nt - 1) / d;
+    auto top_of = [&](int k) { return k == K ? nt - 1 : k * d + d - 2; };
+    std::vector<int4> prog;
+    if (!overlap) {
+        for (int it = nt - 1; it >= 0; --it) {
+            if (!is_stored(it, nt, d)) {
+                int k = it / d, c = k * d;
+                if (it == top_of(k))
+                    for (int itt = c; itt < it; ++itt) prog.push_back(make_int4(K_REP, itt, K_NONE, 0));
+            }
+            prog.push_back(make_int4(K_ADJ, it, K_NONE, 0));
+        }
+        return prog;
+    }
+    std::deque<int2> rq;
+    std::vector<int> need(K + 1, 0), done(K + 1, 0);
+    for (int k = K; k >= 0; --k) {
+        int c = k * d, top = top_of(k);
+        for (int itt = c; itt < top; ++itt) rq.push_back(make_int2(k, itt));
+        need[k] = std::max(0, top - c);
+    }
+    int a = nt - 1;
+    while (!rq.empty() || a >= 0) {
+        int4 item = make_int4(K_NONE, 0, K_NONE, 0);
+        int rep_k = -1;
+        if (!rq.empty()) {
+            int k = rq.front().x;
+            bool ok = (k + 2 > K) || (a <= (k + 2) * d);
+            if (ok) {
+                item.x = K_REP;
+                item.y = rq.front().y;
+                rep_k = k;
+                rq.pop_front();
+            }
+        }
+        if (a >= 0) {
+            bool ok = is_stored(a, nt, d) || done[a / d] >= need[a / d];
+            if (ok) {
+                item.z = K_ADJ;
+                item.w = a;
+                --a;
+            }
+        }
+        if (rep_k >= 0) done[rep_k]++;
+        prog.push_back(item);
+    }
+    return prog;
+}
+
+static int get_program(fwi_ctx *c, const std::string &key, const std::vector<int4> &items, Program **out)
+{
+    auto it = c->progs.find(key);
+    if (it == c->progs.end()) {
+        Program p;
+        p.items = items;
+        TRY(dmalloc(c, (void **)&p.d, items.size() * sizeof(int4)));
+        CK(cudaMemcpy(p.d, items.data(), items.size() * sizeof(int4), cudaMemcpyHostToDevice));
+        it = c->progs.emplace(key, std::move(p)).first;
+    }
+    *out = &it->second;
+    return FWI_OK;
+}
+
+// ---------------------------------------------------------------- launching
+typedef void (*StepFn)(const ShotDesc *, const int4 *, int, int, int);
+
+static void pick_launch(int Nx, int nshot, bool batched, int *lx, StepFn *fn)
+{
+    // blocks = strips x shots x 2; the single-shot path wants many small strips
+    int want = batched ? 32 : 8;
+    if (!batched && Nx / want < 2 * 148) want = 4;
+    (void)nshot;
+    *lx = want;
+    switch (want) {
+    case 4: *fn = k_step<4>; break;
+    case 8: *fn = k_step<8>; break;
+    case 16: *fn = k_step<16>; break;
+    default: *fn = k_step<32>; break;
+    }
+}
+
+static int launch_steps(fwi_ctx *c, const Program *prog, int shot_base, int nshot, int prog_stride, const Plan *p,
+                        bool batched)
+{
+    int lx;
+    StepFn fn;
+    pick_launch(p->Nx, nshot, batched, &lx, &fn);
+    const int W = (p->G + 31) / 32;
+    int threads = 32 * W, zchunks = 1;
+    if (threads > 256) {  // very tall columns: split the column over several blocks
+        zchunks = (threads + 255) / 256;
+        threads = 256;
+    }
+    if (zchunks > 1) return fail(FWI_ERR_UNSUPPORTED, "grid with %d padded rows is taller than one block", p->Nz);
+    dim3 grid((p->Nx + lx - 1) / lx, 2 * nshot, zchunks);
+    const int n = (int)prog->items.size();
+    for (int L = 0; L < n; L++) {
+        const int4 &pw = prog->items[L];
+        if (pw.x == K_NONE && pw.z == K_NONE) continue;
+        fn<<<grid, threads, 0, c->stream>>>(c->d_desc, prog->d, prog_stride, L, shot_base);
+        c->launches++;
+    }
+    CK(cudaGetLastError());
+    return FWI_OK;
+}
+
+static int upload_descs(fwi_ctx *c, const std::vector<ShotDesc> &v)
+{
+    if ((int)v.size() > c->desc_cap) {
+        drop_graphs(c);  // captured launches hold the old descriptor array
+        dfree(c, c->d_desc, 0);
+        c->d_desc = nullptr;
+        c->desc_cap = std::max<int>((int)v.size(), 8);
+        TRY(dmalloc(c, (void **)&c->d_desc, c->desc_cap * sizeof(ShotDesc)));
+    }
+    CK(cudaMemcpyAsync(c->d_desc, v.data(), v.size() * sizeof(ShotDesc), cudaMemcpyHostToDevice, c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+    return FWI_OK;
+}
+
+static int scratch(fwi_ctx *c, size_t bytes, void **out)
+{
+    if (bytes > c->scratch_cap) {
+        dfree(c, c->d_scratch, 0);
+        c->d_scratch = nullptr;
+        c->scratch_cap = std::max<size_t>(bytes, 1 << 16);
+        TRY(dmalloc(c, &c->d_scratch, c->scratch_cap));
+    }
+    *out = c->d_scratch;
+    return FWI_OK;
+}
+
+// small descriptor arrays go through a pinned staging copy on the stream
+template <class T>
+static int put(fwi_ctx *c, const std::vector<T> &v, T **dev, size_t offset_bytes)
+{
+    void *base;
+    TRY(scratch(c, offset_bytes + v.size() * sizeof(T) + 256, &base));
+    *dev = (T *)((char *)base + offset_bytes);
+    CK(cudaMemcpyAsync(*dev, v.data(), v.size() * sizeof(T), cudaMemcpyHostToDevice, c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+    return FWI_OK;
+}
+
+static int ensure_red(fwi_ctx *c)
+{
+    if (!c->d_red) TRY(dmalloc(c, (void **)&c->d_red, (size_t)(2 * 1024 + 4096) * 8 * 64));
+    return FWI_OK;
+}
+
+// FP64 sums of several arrays: results in out_host (2 per descriptor)
+static int reduce(fwi_ctx *c, std::vector<SumDesc> sd, std::vector<double> &out_host, double **out_dev = nullptr)
+{
+    TRY(ensure_red(c));
+    const int NP = 592;  // partials per array: 4 per SM
+    const int nd = (int)sd.size();
+    if (nd > 64) return fail(FWI_ERR_ARG, "too many reduction operands");
+    for (int i = 0; i < nd; i++) sd[i].partial = c->d_red + (size_t)i * 2 * NP;
+    double *res = c->d_red + (size_t)64 * 2 * NP;
+    SumDesc *d;
+    TRY(put(c, sd, &d, 0));
+    k_sum_partial<256><<<dim3(NP, nd), 256, 0, c->stream>>>(d);
+    k_sum_final<<<nd, 32, 0, c->stream>>>(d, NP, res);
+    c->launches += 2;
+    CK(cudaGetLastError());
+    if (out_dev) *out_dev = res;
+    out_host.resize(2 * nd);
+    CK(cudaMemcpyAsync(out_host.data(), res, 2 * nd * 8, cudaMemcpyDeviceToHost, c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+    return FWI_OK;
+}
+
+// ---------------------------------------------------------------- runs
+static int gather(fwi_ctx *c, const std::vector<ShotRun *> &rs, int mode, bool with_adj)
+{
+    std::vector<GatherDesc> gd;
+    int maxns = 1, maxtr = 1;
+    for (ShotRun *r : rs) {
+        GatherDesc g;
+        g.traces_t = r->d.traces_t;
+        g.pre = c->d_pre[r->shot];
+        g.obs = c->d_obs[r->shot];
+        g.adj_t = with_adj ? (float *)r->d.adj_t : nullptr;
+        g.tct = r->d_tct;
+        g.tcr = r->d_tcr;
+        g.ns = r->d.ns;
+        g.ntr = r->d.ntr;
+        g.Lt = mode == 1 ? r->Lt : 0;
+        g.Lr = mode == 1 ? r->Lr : 0;
+        g.adj_rows = c->nt;
+        gd.push_back(g);
+        maxns = std::max(maxns, g.ns);
+        maxtr = std::max(maxtr, g.ntr);
+    }
+    GatherDesc *d;
+    TRY(put(c, gd, &d, 0));
+    dim3 grid((maxns + 31) / 32, (maxtr + 31) / 32, (unsigned)gd.size());
+    k_gather<<<grid, dim3(32, 8), 0, c->stream>>>(d, mode);
+    c->launches++;
+    CK(cudaGetLastError());
+    return FWI_OK;
+}
+
+static int finalize(fwi_ctx *c, const std::vector<ShotRun *> &rs, int which)
+{
+    std::vector<FinDesc> fd;
+    for (ShotRun *r : rs) {
+        FinDesc f;
+        f.acc = which == 0 ? r->d.H : r->d.Gacc;
+        f.out = which == 0 ? r->d_hshot : r->d_gshot;
+        f.vp = c->d_vp;
+        f.rho = c->d_rho;
+        f.ix_min = c->shots[r->shot].s.ix_min;
+        f.nxx = r->d.nxx;
+        f.nz = c->nz;
+        f.pml = c->pml;
+        f.ld = r->d.ld;
+        fd.push_back(f);
+    }
+    FinDesc *d;
+    TRY(put(c, fd, &d, 0));
+    k_finalize<<<dim3(148, (unsigned)fd.size()), 256, 0, c->stream>>>(d, which);
+    c->launches++;
+    CK(cudaGetLastError());
+    return FWI_OK;
+}
+
+static int shot_precondition(fwi_ctx *c, const std::vector<ShotRun *> &rs)
+{
+    std::vector<SumDesc> sd;
+    for (ShotRun *r : rs) {
+        SumDesc s{};
+        s.a = r->d_hshot;
+        s.n = (long long)r->d.nxx * c->nz;
+        s.op = 0;
+        sd.push_back(s);
+    }
+    std::vector<double> h;
+    double *res;
+    for (size_t i0 = 0; i0 < sd.size(); i0 += 64) {
+        std::vector<SumDesc> part(sd.begin() + i0, sd.begin() + std::min(sd.size(), i0 + 64));
+        TRY(reduce(c, part, h, &res));
+        std::vector<PrecDesc> pd;
+        for (size_t i = 0; i < part.size(); i++) {
+            ShotRun *r = rs[i0 + i];
+            PrecDesc p;
+            p.g = r->d_gshot;
+            p.h = r->d_hshot;
+            p.n = part[i].n;
+            p.sum = res + 2 * i;
+            pd.push_back(p);
+        }
+        PrecDesc *d;
+        TRY(put(c, pd, &d, 4096));
+        k_shot_precondition<<<dim3(148, (unsigned)pd.size()), 256, 0, c->stream>>>(d);
+        c->launches++;
+        CK(cudaGetLastError());
+        CK(cudaStreamSynchronize(c->stream));
+    }
+    return FWI_OK;
+}
+
+static int stack_and_precondition(fwi_ctx *c, const std::vector<ShotRun *> &rs, int precondition)
+{
+    const long long m = (long long)c->nz * c->nx;
+    CK(cudaMemsetAsync(c->d_gc, 0, m * 8, c->stream));
+    CK(cudaMemsetAsync(c->d_hc, 0, m * 8, c->stream));
+    std::vector<StackShot> ss;
+    for (ShotRun *r : rs) {
+        StackShot s;
+        s.g = r->d_gshot;
+        s.h = r->d_hshot;
+        s.ix_min = c->shots[r->shot].s.ix_min;
+        s.ix_max = c->shots[r->shot].s.ix_max;
+        ss.push_back(s);
+    }
+    StackShot *d;
+    TRY(put(c, ss, &d, 0));
+    k_stack<<<592, 256, 0, c->stream>>>(d, (int)ss.size(), c->nz, c->nx, precondition == 1, c->d_gc, c->d_hc);
+    k_to_float<<<592, 256, 0, c->stream>>>(c->d_gc, c->d_grad, m);
+    c->launches += 2;
+    if (precondition == 1) {
+        k_to_float<<<592, 256, 0, c->stream>>>(c->d_hc, c->d_prec, m);
+        SumDesc s{};
+        s.a = c->d_prec;
+        s.n = m;
+        s.op = 2;
+        std::vector<double> h;
+        double *res;
+        TRY(reduce(c, {s}, h, &res));
+        k_global_precondition<<<592, 256, 0, c->stream>>>(c->d_grad, c->d_prec, m, res, 0.005f);
+        c->launches += 2;
+    }
+    CK(cudaGetLastError());
+    return FWI_OK;
+}
+
+// zero the frames a pass reads before it has written them
+static int zero_initial(fwi_ctx *c, ShotRun *r, bool gradient)
+{
+    const size_t fb = (size_t)r->d.frame * 4;
+    CK(cudaMemsetAsync(r->d.fscr, 0, 3 * fb, c->stream));
+    if (gradient) {
+        CK(cudaMemsetAsync(r->d.ckslots, 0, 2 * fb, c->stream));  // u(-1), u(0)
+        CK(cudaMemsetAsync(r->d.H, 0, (size_t)r->d.frame * 8, c->stream));
+        CK(cudaMemsetAsync(r->d.Gacc, 0, (size_t)r->d.frame * 8, c->stream));
+    }
+    return FWI_OK;
+}
+
+// A(nt) = 0 and A(nt-1) = -injection(nt-1) (propagation.c:676-682 applied to the zero field)
+__global__ void k_adj_init(const ShotDesc *__restrict__ shots, int shot_base)
+{
+    const ShotDesc &S = shots[shot_base + blockIdx.x];
+    if (threadIdx.x != 0) return;
+    float *A = adj_buf(S, S.nt - 1);
+    const float *arow = S.adj_t + (long long)(S.nt - 1) * S.ntr;
+    for (int x = 0; x < S.Nx; x++)
+        for (int e = S.colptr[x]; e < S.colptr[x + 1]; e++) {
+            int2 rr = S.rec[e];
+            float a = __fmul_rn(__fmul_rn(__fmul_rn(__fmul_rn(__fmul_rn(arow[rr.y], S.recK[e]), S.dt), S.dt), S.invdx), S.invdz);
+            float *cell = A + (long long)x * S.ld + rr.x;
+            *cell = __fsub_rn(*cell, a);
+        }
+}
+
+static int adj_init(fwi_ctx *c, const std::vector<ShotRun *> &rs, int shot_base)
+{
+    for (ShotRun *r : rs) {
+        const size_t fb = (size_t)r->d.frame * 4;
+        CK(cudaMemsetAsync(adj_buf(r->d, c->nt - 1), 0, fb, c->stream));
+        CK(cudaMemsetAsync(adj_buf(r->d, c->nt), 0, fb, c->stream));
+    }
+    k_adj_init<<<(unsigned)rs.size(), 32, 0, c->stream>>>(c->d_desc, shot_base);
+    c->launches++;
+    CK(cudaGetLastError());
+    return FWI_OK;
+}
+
+// run a program over a group of shots, through a cached CUDA graph on the batched path
+static int run_program(fwi_ctx *c, const std::string &key, const Program *prog, int shot_base, int nshot,
+                       const Plan *p, bool batched)
+{
+    if (!batched) return launch_steps(c, prog, shot_base, nshot, 0, p, false);
+    auto it = c->graphs.find(key);
+    if (it == c->graphs.end()) {
+        cudaGraph_t g;
+        CK(cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal));
+        long long before = c->launches;
+        int rc = launch_steps(c, prog, shot_base, nshot, 0, p, true);
+        cudaError_t e = cudaStreamEndCapture(c->stream, &g);
+        if (rc != FWI_OK) return rc;
+        if (e != cudaSuccess) return fail(FWI_ERR_CUDA, "graph capture: %s", cudaGetErrorString(e));
+        cudaGraphExec_t ge;
+        e = cudaGraphInstantiate(&ge, g, 0);
+        cudaGraphDestroy(g);
+        if (e != cudaSuccess) return fail(FWI_ERR_CUDA, "graph instantiate: %s", cudaGetErrorString(e));
+        c->launches = before;
+        it = c->graphs.emplace(key, ge).first;
+    }
+    CK(cudaGraphLaunch(it->second, c->stream));
+    c->stats.graph_launches++;
+    // count the kernels the graph holds
+    for (const int4 &pw : prog->items)
+        if (pw.x != K_NONE || pw.z != K_NONE) c->launches++;
+    return FWI_OK;
+}
+
+static int run_forward_group(fwi_ctx *c, std::vector<ShotRun *> &rs, int problem, float freq, int filter, bool batched,
+                             const std::string &gkey, int shot_base)
+{
+    Program *prog;
+    TRY(get_program(c, "fwd0", program_forward(c->nt, K_FWD0), &prog));
+    for (ShotRun *r : rs) TRY(zero_initial(c, r, false));
+    TRY(run_program(c, "fwd0/" + gkey, prog, shot_base, (int)rs.size(), rs[0]->plan, batched));
+    if (problem == 2) {
+        if (filter == 0 || filter == 1) return fail(FWI_ERR_UNSUPPORTED, "residual filter %d (FFT) is not built", filter);
+        for (ShotRun *r : rs) TRY(prepare_taper(c, r, freq));
+    }
+    TRY(gather(c, rs, problem == 2 ? 1 : 0, false));
+    return FWI_OK;
+}
+
+static int run_gradient_group(fwi_ctx *c, std::vector<ShotRun *> &rs, float freq, int filter, int precondition,
+                              bool batched, const std::string &gkey, int shot_base)
+{
+    if (filter == 0 || filter == 1) return fail(FWI_ERR_UNSUPPORTED, "residual filter %d (FFT) is not built", filter);
+    for (ShotRun *r : rs)
+        if (r->d.sr > 1) return fail(FWI_ERR_UNSUPPORTED, "sampleRate > 1 needs FFT trace interpolation (not built)");
+    Program *pf, *pa;
+    TRY(get_program(c, "fwd1", program_forward(c->nt, K_FWD1), &pf));
+    TRY(get_program(c, batched ? "adj/overlap" : "adj/plain", program_adjoint(c->nt, batched), &pa));
+    for (ShotRun *r : rs) TRY(zero_initial(c, r, true));
+    TRY(run_program(c, "fwd1/" + gkey, pf, shot_base, (int)rs.size(), rs[0]->plan, batched));
+    if (precondition == 1) TRY(finalize(c, rs, 0));
+    for (ShotRun *r : rs) TRY(prepare_taper(c, r, freq));
+    TRY(gather(c, rs, 1, true));
+    TRY(adj_init(c, rs, shot_base));
+    TRY(run_program(c, std::string(batched ? "adjo/" : "adjp/") + gkey, pa, shot_base, (int)rs.size(), rs[0]->plan,
+                    batched));
+    TRY(finalize(c, rs, 1));
+    if (precondition == 1) TRY(shot_precondition(c, rs));
+    return FWI_OK;
+}
+
+extern "C" int fwi_ctx_run(fwi_ctx *c, int problem, float freq, int filter, int precondition, int path)
+{
+    if (!c) return fail(FWI_ERR_ARG, "NULL context");
+    if (problem < 0 || problem > 2) return fail(FWI_ERR_ARG, "problem must be 0, 1 or 2 (got %d)", problem);
+    if (c->shots.empty()) return fail(FWI_ERR_STATE, "no shots");
+    CK(cudaSetDevice(c->device));
+    const bool batched = path == FWI_PATH_BATCHED;
+    const bool gradient = problem == 1;
+    const int ns = (int)c->shots.size();
+    long long launches0 = c->launches;
+    double cells = 0.0;
+    CK(cudaEventRecord(c->ev0, c->stream));
+    if (batched) {
+        // one group per plan geometry: shots sharing a window run in the same launches
+        if ((int)c->runs.size() != ns) {
+            free_runs(c);
+            for (int i = 0; i < ns; i++) c->runs.emplace_back(new ShotRun());
+        }
+        std::vector<ShotDesc> descs(ns);
+        for (int i = 0; i < ns; i++) {
+            TRY(prepare_run(c, c->runs[i].get(), i, gradient));
+            c->runs[i]->d.hessian = gradient && precondition == 1;
+        }
+        // group consecutive shots with the same plan
+        std::vector<std::pair<int, int>> groups;
+        for (int i = 0; i < ns; i++) {
+            if (groups.empty() || c->runs[i]->plan != c->runs[groups.back().first]->plan) groups.push_back({i, 1});
+            else groups.back().second++;
+        }
+        for (int i = 0; i < ns; i++) descs[i] = c->runs[i]->d;
+        TRY(upload_descs(c, descs));
+        for (auto &gr : groups) {
+            std::vector<ShotRun *> rs;
+            for (int i = gr.first; i < gr.first + gr.second; i++) rs.push_back(c->runs[i].get());
+            std::string gkey = std::to_string(gr.first) + "+" + std::to_string(gr.second) + "@" +
+                               std::to_string((long long)(intptr_t)rs[0]->plan);
+            if (gradient) TRY(run_gradient_group(c, rs, freq, filter, precondition, true, gkey, gr.first));
+            else TRY(run_forward_group(c, rs, problem, freq, filter, true, gkey, gr.first));
+        }
+        if (gradient) {
+            std::vector<ShotRun *> all;
+            for (auto &r : c->runs) all.push_back(r.get());
+            TRY(stack_and_precondition(c, all, precondition));
+        }
+    } else {
+        // plain: one shot state, shots in sequence (propagation.c:857, :895)
+        if (c->runs.size() != 1) {
+            free_runs(c);
+            c->runs.emplace_back(new ShotRun());
+        }
+        ShotRun *r = c->runs[0].get();
+        std::vector<float *> gsh, hsh;
+        std::vector<std::unique_ptr<ShotRun>> keep;  // per-shot gradient copies for the stack
+        std::vector<ShotRun *> stack_list;
+        for (int i = 0; i < ns; i++) {
+            TRY(prepare_run(c, r, i, gradient));
+            r->d.hessian = gradient && precondition == 1;
+            TRY(upload_descs(c, {r->d}));
+            std::vector<ShotRun *> rs = {r};
+            if (gradient) {
+                TRY(run_gradient_group(c, rs, freq, filter, precondition, false, "", 0));
+                // keep this shot's FP32 gradient / preconditioner for the stack
+                std::unique_ptr<ShotRun> k(new ShotRun());
+                k->shot = i;
+                size_t m = (size_t)c->nz * r->d.nxx * 4;
+                void *q;
+                TRY(ralloc(c, k.get(), &q, m)); k->d_gshot = (float *)q;
+                TRY(ralloc(c, k.get(), &q, m)); k->d_hshot = (float *)q;
+                CK(cudaMemcpyAsync(k->d_gshot, r->d_gshot, m, cudaMemcpyDeviceToDevice, c->stream));
+                CK(cudaMemcpyAsync(k->d_hshot, r->d_hshot, m, cudaMemcpyDeviceToDevice, c->stream));
+                stack_list.push_back(k.get());
+                keep.push_back(std::move(k));
+            } else {
+                TRY(run_forward_group(c, rs, problem, freq, filter, false, "", 0));
+            }
+            CK(cudaStreamSynchronize(c->stream));
+        }
+        if (gradient) TRY(stack_and_precondition(c, stack_list, precondition));
+        CK(cudaStreamSynchronize(c->stream));
+        for (auto &k : keep) free_run(c, k.get());
+    }
+    CK(cudaEventRecord(c->ev1, c->stream));
+    CK(cudaEventSynchronize(c->ev1));
+    float ms = 0.f;
+    CK(cudaEventElapsedTime(&ms, c->ev0, c->ev1));
+    for (int i = 0; i < ns; i++) {
+        const fwi_shot &s = c->shots[i].s;
+        double cellsz = (double)(c->nz + 2 * c->pml) * (s.ix_max - s.ix_min + 1 + 2 * c->pml);
+        int d = fwi_ck_interval(c->nt);
+        double steps = gradient ? (double)c->nt * 2 + (c->nt - fwi_ck_count(c->nt)) : (double)c->nt;
+        (void)d;
+        cells += cellsz * steps;
+    }
+    c->stats.ms = ms;
+    c->stats.cell_updates = cells;
+    c->stats.kernel_launches = c->launches - launches0;
+    c->stats.device_bytes = c->used;
+    return FWI_OK;
+}
+
+extern "C" int fwi_ctx_get_traces(fwi_ctx *c, int ishot, float *out)
+{
+    if (!c || !out || ishot < 0 || ishot >= (int)c->shots.size()) return fail(FWI_ERR_ARG, "bad shot index %d", ishot);
+    CK(cudaSetDevice(c->device));
+    const fwi_shot &s = c->shots[ishot].s;
+    CK(cudaMemcpyAsync(out, c->d_pre[ishot], (size_t)s.ntr * s.ns * 4, cudaMemcpyDeviceToHost, c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+    return FWI_OK;
+}
+
+extern "C" int fwi_ctx_get_gradient(fwi_ctx *c, float *out)
+{
+    if (!c || !out) return fail(FWI_ERR_ARG, "NULL argument");
+    CK(cudaSetDevice(c->device));
+    CK(cudaMemcpyAsync(out, c->d_grad, (size_t)c->nz * c->nx * 4, cudaMemcpyDeviceToHost, c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+    return FWI_OK;
+}
+
+extern "C" const float *fwi_ctx_traces_device(fwi_ctx *c, int ishot)
+{
+    if (!c || ishot < 0 || ishot >= (int)c->shots.size()) return nullptr;
+    return c->d_pre[ishot];
+}
+extern "C" const float *fwi_ctx_gradient_device(fwi_ctx *c) { return c ? c->d_grad : nullptr; }
+
+extern "C" int fwi_ctx_objective(fwi_ctx *c, double *out)
+{
+    if (!c || !out) return fail(FWI_ERR_ARG, "NULL argument");
+    CK(cudaSetDevice(c->device));
+    double acc = 0.0;
+    std::vector<SumDesc> sd;
+    for (size_t i = 0; i < c->shots.size(); i++) {
+        SumDesc s{};
+        s.a = c->d_pre[i];
+        s.n = (long long)c->shots[i].s.ntr * c->shots[i].s.ns;
+        s.op = 1;
+        sd.push_back(s);
+    }
+    for (size_t i0 = 0; i0 < sd.size(); i0 += 64) {
+        std::vector<SumDesc> part(sd.begin() + i0, sd.begin() + std::min(sd.size(), i0 + 64));
+        std::vector<double> h;
+        TRY(reduce(c, part, h));
+        for (size_t i = 0; i < part.size(); i++) acc += h[2 * i];
+    }
+    *out = 0.5 * acc;
+    return FWI_OK;
+}
+
+extern "C" int fwi_ctx_stats(fwi_ctx *c, fwi_stats *out)
+{
+    if (!c || !out) return fail(FWI_ERR_ARG, "NULL argument");
+    *out = c->stats;
+    return FWI_OK;
+}

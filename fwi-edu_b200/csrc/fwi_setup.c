@@ -1,0 +1,235 @@
+/*
+ * fwi_setup.c -- host-side per-model set-up of the B200 engine.
+ *
+ * Builds the coefficient fields the device stencil streams: pad the model window
+ * (pad_model2d, common.c:110-176), build the MEAL damping D and scale Beta
+ * (mealCoefs2d, propagation.c:192-354), fold them into the model and the time
+ * coefficients (propagation.c:513-529), then K, 1/rho and its derivatives
+ * (acoustic_iso2d_rgfd_parameter, propagation.c:103-171, with the two-point edge
+ * derivative of calculate_gradient2d, common.c:416-479).
+ *
+ * This runs once per (model window, peak frequency) and stays on the host on
+ * purpose: the reference evaluates these fields with the C library's expf, logf
+ * and powf and rounds double expressions to float at fixed points, and keeping
+ * the same operation order here with the same libm gives identical coefficient
+ * bits, which is what lets the device stencil reproduce the reference exactly.
+ * The file is compiled with -O2 -fno-fast-math -ffp-contract=off.
+ */
+#include <math.h>
+#include <stdlib.h>
+#include <string.h>
+#include "fwi_setup.h"
+
+#define AT(a, ix, iz, n1) (a)[(size_t)(ix) * (size_t)(n1) + (size_t)(iz)]
+
+static float *falloc(size_t n)
+{
+    void *p = NULL;
+    if (posix_memalign(&p, 64, (n ? n : 1) * sizeof(float))) return NULL;
+    memset(p, 0, (n ? n : 1) * sizeof(float));
+    return (float *)p;
+}
+
+int fwi_ck_interval(int nt)
+{
+    float r = roundf(sqrtf(2.0f * (nt - 1)));
+    return (int)(r > 3.0f ? r : 3.0f);
+}
+
+int fwi_ck_count(int nt)
+{
+    int d = fwi_ck_interval(nt), n = 0;
+    for (int it = 0; it < nt; it++) n += (it % d == 0 || (it + 1) % d == 0);
+    return n;
+}
+
+double fwi_src_term_f64(float src, float K, float dt, float invdx, float invdz)
+{
+    return 1.0 * src * K * dt * dt * invdx * invdz;
+}
+
+float fwi_src_term_f32(float src, float K, float dt, float invdx, float invdz)
+{
+    return src * K * dt * dt * invdx * invdz;
+}
+
+void fwi_taper_coefs(int L, float *out)
+{
+    for (int i = 0; i <= L; i++) {
+        float x = (float)3.141592653589793 * i / L;
+        out[i] = 0.5f * (1.0f + cosf(x));
+    }
+}
+
+/* the absorbing-layer weight of layer l of n: 2^(d^alpha) - 1, d = l/n (propagation.c:173-190) */
+static float layer_weight(float alpha, int l, int n)
+{
+    float d = (0.1f * l) / (0.1f * n);
+    return expf(logf(2.0f) * powf(d, alpha)) - 1.0f;
+}
+
+void fwi_free_coefs(fwi_coefs *c)
+{
+    free(c->c1); free(c->c2); free(c->ck); free(c->irx); free(c->irz); free(c->ir); free(c->K);
+    memset(c, 0, sizeof(*c));
+}
+
+int fwi_setup_coefs(const float *vpm, const float *rhom, int nz, int nxx, int pml, float dx, float dz,
+                    float dt, float fpeak, fwi_coefs *o)
+{
+    memset(o, 0, sizeof(*o));
+    const int Nz = nz + 2 * pml, Nx = nxx + 2 * pml, nl = pml;
+    const size_t n = (size_t)Nz * Nx;
+    o->nz = nz; o->nxx = nxx; o->pml = pml; o->Nz = Nz; o->Nx = Nx;
+    o->ld = (Nz + 3) & ~3;
+    o->invdx = 1.0f / dx;
+    o->invdz = 1.0f / dz;
+    o->invdxdx = 1.0f / (dx * dx);
+    o->invdzdz = 1.0f / (dz * dz);
+    o->invdtdt = 1.0f / (dt * dt);
+
+    float *vp = falloc(n), *rho = falloc(n), *Dx = falloc(n), *Dz = falloc(n), *Bx = falloc(n), *Bz = falloc(n);
+    float *K = falloc(n), *ir = falloc(n), *irx = falloc(n), *irz = falloc(n);
+    size_t nl_out = (size_t)o->ld * Nx;
+    o->c1 = falloc(nl_out); o->c2 = falloc(nl_out); o->ck = falloc(nl_out);
+    o->irx = falloc(nl_out); o->irz = falloc(nl_out); o->ir = falloc(nl_out); o->K = falloc(nl_out);
+    if (!vp || !rho || !Dx || !Dz || !Bx || !Bz || !K || !ir || !irx || !irz || !o->c1 || !o->c2 || !o->ck ||
+        !o->irx || !o->irz || !o->ir || !o->K) {
+        free(vp); free(rho); free(Dx); free(Dz); free(Bx); free(Bz); free(K); free(ir); free(irx); free(irz);
+        fwi_free_coefs(o);
+        return -1;
+    }
+
+    /* edge-replicating pad: interior, then top, bottom, left, right */
+    for (int ix = 0; ix < nxx; ix++)
+        for (int iz = 0; iz < nz; iz++) {
+            AT(vp, ix + nl, iz + nl, Nz) = AT(vpm, ix, iz, nz);
+            AT(rho, ix + nl, iz + nl, Nz) = AT(rhom, ix, iz, nz);
+        }
+    for (int ix = 0; ix < Nx; ix++) {
+        for (int iz = 0; iz < nl; iz++) {
+            AT(vp, ix, iz, Nz) = AT(vp, ix, nl, Nz);
+            AT(rho, ix, iz, Nz) = AT(rho, ix, nl, Nz);
+        }
+        for (int iz = nz + nl; iz < Nz; iz++) {
+            AT(vp, ix, iz, Nz) = AT(vp, ix, nz + nl - 1, Nz);
+            AT(rho, ix, iz, Nz) = AT(rho, ix, nz + nl - 1, Nz);
+        }
+    }
+    for (int ix = 0; ix < nl; ix++)
+        for (int iz = 0; iz < Nz; iz++) {
+            AT(vp, ix, iz, Nz) = AT(vp, nl, iz, Nz);
+            AT(rho, ix, iz, Nz) = AT(rho, nl, iz, Nz);
+        }
+    for (int ix = nxx + nl; ix < Nx; ix++)
+        for (int iz = 0; iz < Nz; iz++) {
+            AT(vp, ix, iz, Nz) = AT(vp, nxx + nl - 1, iz, Nz);
+            AT(rho, ix, iz, Nz) = AT(rho, nxx + nl - 1, iz, Nz);
+        }
+
+    /* MEAL: per-side damping and scale; both default to 0 and 1 outside the layers */
+    for (size_t i = 0; i < n; i++) { Bx[i] = 1.0f; Bz[i] = 1.0f; }
+    const float pd = 2.0f, alpha = 2.5f, ppw_fd = 10.0f;
+    const float Rcoef = powf(10.0f, -1.0f * ((log10f(nl) - 1.0f) / (log10f(2.0f))) - 3.0f - 0.5f * pd);
+    const float logR = logf(Rcoef), s3 = sqrtf(3.0f);
+    const float thick_x = nl * dx, thick_z = nl * dz;
+    for (int ix = 0; ix < Nx; ix++)
+        for (int l = 1; l <= nl; l++) {
+            float w = layer_weight(alpha, l, nl);
+            int zs[2] = {nl - l, Nz - nl - 1 + l}; /* top then bottom: the bottom write wins on overlap */
+            for (int k = 0; k < 2; k++) {
+                int iz = zs[k];
+                float v = AT(vp, ix, iz, Nz);
+                float d0 = -1.0f * (1.0f + pd) * v * logR / (2.0f * thick_z);
+                float ppw = (v / s3) / (dz * fpeak);
+                float beta = 2.0f * ppw / ppw_fd;
+                AT(Dz, ix, iz, Nz) = d0 * w;
+                AT(Bz, ix, iz, Nz) = 1.0f + (beta - 1.0f) * w;
+            }
+        }
+    for (int l = 1; l <= nl; l++) {
+        float w = layer_weight(alpha, l, nl);
+        for (int iz = 0; iz < Nz; iz++) {
+            int xs[2] = {nl - l, Nx - nl - 1 + l}; /* left then right */
+            for (int k = 0; k < 2; k++) {
+                int ix = xs[k];
+                float v = AT(vp, ix, iz, Nz);
+                float d0 = -1.0f * (1.0f + pd) * v * logR / (2.0f * thick_x);
+                float ppw = (v / s3) / (dx * fpeak);
+                float beta = 2.0f * ppw / ppw_fd;
+                AT(Dx, ix, iz, Nz) = d0 * w;
+                AT(Bx, ix, iz, Nz) = 1.0f + (beta - 1.0f) * w;
+            }
+        }
+    }
+
+    /* combine, fold into the model, time coefficients formed in double and rounded to float.
+     * Away from the layers Dx = Dz = 0 and Bx = Bz = 1 exactly, so D = 0, Beta = 1 and the
+     * expressions reduce exactly to coef1 = 2, coef2 = -1, coef3 = dt*dt: no libm call needed there. */
+    const float dtdt = dt * dt;
+    const int ld = o->ld;
+    for (int ix = 0; ix < Nx; ix++) {
+        int xband = ix < nl || ix >= Nx - nl;
+        for (int iz = 0; iz < Nz; iz++) {
+            size_t i = (size_t)ix * Nz + iz;
+            float c1, c2, c3;
+            if (xband || iz < nl || iz >= Nz - nl) {
+                float D = sqrtf(powf(Dx[i], 2.0f) + powf(Dz[i], 2.0f));
+                float B = sqrtf(powf(Bx[i] - 1.0f, 2.0f) + powf(Bz[i] - 1.0f, 2.0f)) + 1.0f;
+                D /= B;
+                vp[i] /= B;
+                rho[i] *= B;
+                c1 = (float)((2.0 - dt * dt * D * D) / (1.0 + dt * D));
+                c2 = (float)(-1.0 * (1.0 - dt * D) / (1.0 + dt * D));
+                c3 = (float)((dt * dt) / (1.0 + dt * D));
+            } else {
+                c1 = 2.0f;
+                c2 = -1.0f;
+                c3 = (float)((double)dtdt / 1.0);
+            }
+            AT(o->c1, ix, iz, ld) = c1;
+            AT(o->c2, ix, iz, ld) = c2;
+            Dx[i] = c3; /* Dx is free from here on: keep coef3 until K is known */
+        }
+    }
+
+    /* K, 1/rho and d(1/rho)/dx, d(1/rho)/dz: two-point at the edges, 12-point optimised inside */
+    for (size_t i = 0; i < n; i++) {
+        K[i] = rho[i] * vp[i] * vp[i];
+        ir[i] = 1.0f / rho[i];
+    }
+    for (int ix = 0; ix < Nx; ix++)
+        for (int iz = 0; iz < Nz; iz++) {
+            size_t i = (size_t)ix * Nz + iz;
+            if (ix == 0) irx[i] = (ir[i + Nz] - ir[i]) / dx;
+            else if (ix == Nx - 1) irx[i] = (ir[i] - ir[i - Nz]) / dx;
+            else irx[i] = (ir[i + Nz] - ir[i - Nz]) / (2.0f * dx);
+            if (iz == 0) irz[i] = (ir[i + 1] - ir[i]) / dz;
+            else if (iz == Nz - 1) irz[i] = (ir[i] - ir[i - 1]) / dz;
+            else irz[i] = (ir[i + 1] - ir[i - 1]) / (2.0f * dz);
+        }
+    const float G1 = 0.91067892f, G2 = -0.34187892f, G3 = 0.13833962f;
+    const float G4 = -0.04880710f, G5 = 0.01302148f, G6 = -0.00199047f;
+    for (int ix = 6; ix < Nx - 6; ix++)
+        for (int iz = 6; iz < Nz - 6; iz++) {
+            size_t i = (size_t)ix * Nz + iz;
+            const float *r = ir + i;
+            irx[i] = (G1 * (r[Nz] - r[-Nz]) + G2 * (r[2 * Nz] - r[-2 * Nz]) + G3 * (r[3 * Nz] - r[-3 * Nz]) +
+                      G4 * (r[4 * Nz] - r[-4 * Nz]) + G5 * (r[5 * Nz] - r[-5 * Nz]) + G6 * (r[6 * Nz] - r[-6 * Nz])) *
+                     o->invdx;
+            irz[i] = (G1 * (r[1] - r[-1]) + G2 * (r[2] - r[-2]) + G3 * (r[3] - r[-3]) + G4 * (r[4] - r[-4]) +
+                      G5 * (r[5] - r[-5]) + G6 * (r[6] - r[-6])) *
+                     o->invdz;
+        }
+    for (int ix = 0; ix < Nx; ix++)
+        for (int iz = 0; iz < Nz; iz++) {
+            size_t i = (size_t)ix * Nz + iz;
+            AT(o->ck, ix, iz, ld) = Dx[i] * K[i];
+            AT(o->ir, ix, iz, ld) = ir[i];
+            AT(o->irx, ix, iz, ld) = irx[i];
+            AT(o->irz, ix, iz, ld) = irz[i];
+            AT(o->K, ix, iz, ld) = K[i];
+        }
+    free(vp); free(rho); free(Dx); free(Dz); free(Bx); free(Bz); free(K); free(ir); free(irx); free(irz);
+    return 0;
+}

@@ -1,0 +1,40 @@
+/* fwi_setup.h -- host-side per-model set-up of the B200 engine (internal). */
+#ifndef FWI_SETUP_H
+#define FWI_SETUP_H
+
+#include <stddef.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* Coefficient fields of one padded model window, in the device layout:
+ * Nx columns of ld floats (ld = Nz rounded up to a multiple of 4), z fastest,
+ * rows Nz..ld-1 zero.  ck = coef3*K (the reference multiplies coef3 by K first). */
+typedef struct {
+    int nz, nxx, pml, Nz, Nx, ld;
+    float *c1, *c2, *ck, *irx, *irz, *ir; /* Nx*ld each, 64-byte aligned */
+    float *K;                              /* Nx*ld, bulk modulus of the beta-scaled model */
+    float invdx, invdz, invdxdx, invdzdz, invdtdt;
+} fwi_coefs;
+
+/* vpm, rhom: the window [nxx][nz] of the model.  Returns 0 or -1 (allocation). */
+int fwi_setup_coefs(const float *vpm, const float *rhom, int nz, int nxx, int pml, float dx, float dz,
+                    float dt, float fpeak, fwi_coefs *out);
+void fwi_free_coefs(fwi_coefs *c);
+
+/* checkpoint interval and count of checkpoint.c:47 and :66-75 */
+int fwi_ck_interval(int nt);
+int fwi_ck_count(int nt);
+
+/* forward source term 1.0*src*K*dt*dt*invdx*invdz formed in double (propagation.c:558) */
+double fwi_src_term_f64(float src, float K, float dt, float invdx, float invdz);
+/* replay source / adjoint injection scale src*K*dt*dt*invdx*invdz in float (propagation.c:662, :681) */
+float fwi_src_term_f32(float src, float K, float dt, float invdx, float invdz);
+/* cosine taper coefficients 0.5(1+cos(pi*i/L)), i = 0..L (common.c:826-831) */
+void fwi_taper_coefs(int L, float *out);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -1,0 +1,240 @@
+"""ctypes binding of libfwi_b200.so (the B200 engine) -- the host-side mirror of the
+reference's propagation interface.
+
+Two ways in, as in the C-ABI (include/fwi_b200.h):
+
+* ``propagation(...)`` calls the drop-in ``fwi_iso_acoustic2d_propagation`` with
+  Record2D shot records and host arrays, exactly as acoustic2d_modeling.c and
+  acoustic2d_fwi.c call ``iso_acoustic2d_propagation`` (propagation.h:133-142);
+* ``Context`` wraps the native device-resident API (fwi_ctx_*).
+
+There is no CPU fallback: loading fails loudly when the library or a GPU is missing.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import subprocess
+import threading
+
+import numpy as np
+
+PKG = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+LIB_PATH = os.path.join(PKG, "lib", "libfwi_b200.so")
+CSRC = os.path.join(PKG, "csrc")
+
+FWI_OK, FWI_ERR_ARG, FWI_ERR_CUDA, FWI_ERR_NOMEM, FWI_ERR_UNSUPPORTED, FWI_ERR_NODEVICE, FWI_ERR_STATE = range(7)
+PATH_PLAIN, PATH_BATCHED = 0, 1
+
+_fp = C.POINTER(C.c_float)
+_ip = C.POINTER(C.c_int)
+_fpp = C.POINTER(_fp)
+
+
+class FwiError(RuntimeError):
+    def __init__(self, code, msg):
+        super().__init__(f"status {code}: {msg}")
+        self.code = code
+
+
+class Record2D(C.Structure):
+    """Shot record, layout of observation.h:18-48."""
+    _fields_ = [("shotID", C.c_int), ("sx", C.c_float), ("sz", C.c_float), ("isx", C.c_int),
+                ("isz", C.c_int), ("fpeak", C.c_float), ("src", _fp), ("gx", _fp), ("gz", _fp),
+                ("igx", _ip), ("igz", _ip), ("sampleRate", C.c_int), ("ntr", C.c_int),
+                ("ns", C.c_int), ("dtr", C.c_float), ("dt", C.c_float), ("ix_min", C.c_int),
+                ("ix_max", C.c_int), ("traces_vx", _fpp), ("traces_vz", _fpp), ("traces_p", _fpp),
+                ("precond", _fpp), ("grad", _fpp)]
+
+
+class FwiShot(C.Structure):
+    _fields_ = [("shotID", C.c_int), ("isx", C.c_int), ("isz", C.c_int), ("ntr", C.c_int),
+                ("ns", C.c_int), ("sampleRate", C.c_int), ("ix_min", C.c_int), ("ix_max", C.c_int),
+                ("dt", C.c_float), ("dtr", C.c_float), ("fpeak", C.c_float),
+                ("src", _fp), ("igx", _ip), ("igz", _ip)]
+
+
+class FwiStats(C.Structure):
+    _fields_ = [("ms", C.c_double), ("cell_updates", C.c_double), ("kernel_launches", C.c_longlong),
+                ("graph_launches", C.c_longlong), ("device_bytes", C.c_size_t)]
+
+
+_lib = None
+_lock = threading.Lock()
+
+
+def build(force: bool = False) -> str:
+    """Compile the library in-tree (nvcc, sm_100a)."""
+    if force or not os.path.exists(LIB_PATH):
+        subprocess.run(["make", "-s", "-C", CSRC, "-j4"], check=True)
+    return LIB_PATH
+
+
+def lib():
+    global _lib
+    with _lock:
+        if _lib is None:
+            if not os.path.exists(LIB_PATH):
+                build()
+            L = C.CDLL(LIB_PATH)
+            L.fwi_last_error.restype = C.c_char_p
+            L.fwi_version.restype = C.c_char_p
+            L.fwi_ctx_traces_device.restype = C.c_void_p
+            L.fwi_ctx_gradient_device.restype = C.c_void_p
+            L.calculate_memory_cost_checkpoint.restype = C.c_float
+            _lib = L
+    return _lib
+
+
+def _check(rc):
+    if rc != FWI_OK:
+        raise FwiError(rc, lib().fwi_last_error().decode(errors="replace"))
+
+
+def _f32(a):
+    return np.ascontiguousarray(a, dtype=np.float32)
+
+
+def _i32(a):
+    return np.ascontiguousarray(a, dtype=np.int32)
+
+
+def _ptr(a, t=_fp):
+    return a.ctypes.data_as(t)
+
+
+def rows(a: np.ndarray):
+    """float** view (alloc2float layout) of a C-contiguous (n2, n1) float32 array."""
+    assert a.dtype == np.float32 and a.flags.c_contiguous
+    n2 = a.shape[0]
+    n1 = int(np.prod(a.shape[1:])) if a.ndim > 1 else 1
+    arr = (_fp * max(n2, 1))()
+    base = a.ctypes.data
+    for i in range(n2):
+        arr[i] = C.cast(base + i * n1 * 4, _fp)
+    return arr
+
+
+class _Keep(list):
+    pass
+
+
+def make_records(shots, traces, keep):
+    """Record2D array for the Shot list with the given per-shot (ntr, ns) trace buffers."""
+    recs = (Record2D * len(shots))()
+    for i, s in enumerate(shots):
+        igx, igz, src = _i32(s.igx), _i32(s.igz), _f32(s.src)
+        gx = ((igx + s.ix_min).astype(np.float32) * np.float32(s.dtr)).astype(np.float32)
+        gz = igz.astype(np.float32)
+        rp = rows(traces[i])
+        keep += [igx, igz, src, gx, gz, rp, traces[i]]
+        r = recs[i]
+        r.shotID = s.shotID; r.sx = s.sx; r.sz = s.sz; r.isx = s.isx; r.isz = s.isz; r.fpeak = s.fpeak
+        r.src = _ptr(src); r.gx = _ptr(gx); r.gz = _ptr(gz); r.igx = _ptr(igx, _ip); r.igz = _ptr(igz, _ip)
+        r.sampleRate = s.sampleRate; r.ntr = len(igx); r.ns = s.ns; r.dtr = s.dtr; r.dt = s.dt
+        r.ix_min = s.ix_min; r.ix_max = s.ix_max
+        r.traces_p = C.cast(rp, _fpp)
+    return recs
+
+
+def propagation(vp, rho, shots, dx, dz, dt, nt, pml, fs, freq, filt, precondition, problem,
+                obs=None, pre=None, iteration=1, path: str | None = None):
+    """Drop-in call: iso_acoustic2d_propagation semantics, host arrays in and out.
+    Returns (pre gathers, grad or None)."""
+    L = lib()
+    if path is not None:
+        os.environ["FWI_PATH"] = path
+    vp, rho = _f32(vp), _f32(rho)
+    nx, nz = vp.shape
+    keep = _Keep()
+    obs = [np.zeros((len(s.igx), s.ns), np.float32) if obs is None else _f32(obs[i]).copy()
+           for i, s in enumerate(shots)]
+    pre = [np.zeros((len(s.igx), s.ns), np.float32) if pre is None else _f32(pre[i]).copy()
+           for i, s in enumerate(shots)]
+    ro = make_records(shots, obs, keep)
+    rp = make_records(shots, pre, keep)
+    vpr, rhor = rows(vp), rows(rho)
+    grad = np.zeros((nx, nz), np.float32) if problem == 1 else None
+    gr = rows(grad) if grad is not None else None
+    rc = L.fwi_iso_acoustic2d_propagation(vpr, rhor, ro, len(shots), nz, nx, C.c_float(dx), C.c_float(dz),
+                                          C.c_float(dt), nt, pml, fs, C.c_float(freq), C.c_float(filt),
+                                          precondition, problem, iteration, 0, rp, gr)
+    _check(rc)
+    return pre, grad
+
+
+class Context:
+    """Device-resident engine context (fwi_ctx_*)."""
+
+    def __init__(self, device: int = 0, budget_bytes: int = 0):
+        self.L = lib()
+        self.h = C.c_void_p()
+        _check(self.L.fwi_ctx_create(C.byref(self.h), device, C.c_size_t(budget_bytes)))
+        self._keep = []
+        self.shots = []
+
+    def close(self):
+        if self.h:
+            self.L.fwi_ctx_destroy(self.h)
+            self.h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def set_model(self, vp, rho, dx, dz, dt, nt, pml, fs):
+        vp, rho = _f32(vp), _f32(rho)
+        nx, nz = vp.shape
+        self.nx, self.nz = nx, nz
+        _check(self.L.fwi_ctx_set_model(self.h, _ptr(vp), _ptr(rho), nz, nx, C.c_float(dx), C.c_float(dz),
+                                        C.c_float(dt), nt, pml, fs))
+
+    def set_model_device(self, vp_ptr, rho_ptr, nz, nx, dx, dz, dt, nt, pml, fs):
+        self.nx, self.nz = nx, nz
+        _check(self.L.fwi_ctx_set_model_device(self.h, C.c_void_p(vp_ptr), C.c_void_p(rho_ptr), nz, nx,
+                                               C.c_float(dx), C.c_float(dz), C.c_float(dt), nt, pml, fs))
+
+    def set_shots(self, shots):
+        arr = (FwiShot * len(shots))()
+        keep = []
+        for i, s in enumerate(shots):
+            igx, igz, src = _i32(s.igx), _i32(s.igz), _f32(s.src)
+            keep += [igx, igz, src]
+            a = arr[i]
+            a.shotID = s.shotID; a.isx = s.isx; a.isz = s.isz; a.ntr = len(igx); a.ns = s.ns
+            a.sampleRate = s.sampleRate; a.ix_min = s.ix_min; a.ix_max = s.ix_max
+            a.dt = s.dt; a.dtr = s.dtr; a.fpeak = s.fpeak
+            a.src = _ptr(src); a.igx = _ptr(igx, _ip); a.igz = _ptr(igz, _ip)
+        _check(self.L.fwi_ctx_set_shots(self.h, arr, len(shots)))
+        self.shots = list(shots)
+
+    def set_observed(self, obs):
+        obs = [_f32(o) for o in obs]
+        p = (_fp * len(obs))(*[_ptr(o) for o in obs])
+        _check(self.L.fwi_ctx_set_observed(self.h, p))
+
+    def run(self, problem, freq=0.0, filt=2, precondition=1, path=PATH_BATCHED):
+        _check(self.L.fwi_ctx_run(self.h, problem, C.c_float(freq), filt, precondition, path))
+
+    def traces(self, i):
+        s = self.shots[i]
+        out = np.empty((len(s.igx), s.ns), np.float32)
+        _check(self.L.fwi_ctx_get_traces(self.h, i, _ptr(out)))
+        return out
+
+    def gradient(self):
+        out = np.empty((self.nx, self.nz), np.float32)
+        _check(self.L.fwi_ctx_get_gradient(self.h, _ptr(out)))
+        return out
+
+    def objective(self):
+        v = C.c_double()
+        _check(self.L.fwi_ctx_objective(self.h, C.byref(v)))
+        return v.value
+
+    def stats(self):
+        s = FwiStats()
+        _check(self.L.fwi_ctx_stats(self.h, C.byref(s)))
+        return {k: getattr(s, k) for k, _ in FwiStats._fields_}

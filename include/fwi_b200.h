@@ -1,0 +1,185 @@
+/*
+ * fwi_b200.h -- C-ABI of the B200 (sm_100a) 2-D acoustic forward/adjoint engine.
+ *
+ * Two layers:
+ *
+ * 1. Drop-in entry points with the names, argument meaning and effects of the
+ *    FWI-EDU C implementation (FWILab2dCLangV1.2.6).  A front-end written against
+ *    the reference links against this library instead and runs unchanged.  Each
+ *    declaration cites the reference declaration it replaces.  Where the reference
+ *    calls err() and exits, these print the same kind of message and return; the
+ *    matching fwi_* entry point returns the status code instead.
+ *
+ * 2. The native API (fwi_ctx_*): a device-resident context that keeps the model,
+ *    coefficients, wavelets, traces, checkpoints and gradients in HBM, runs shots
+ *    one per launch ("plain") or many shots per launch ("batched"), and hands
+ *    results back on request.  Plain pointers and sizes only.
+ *
+ * Array layout everywhere: the reference's alloc2float(n1, n2) layout -- n2 rows of
+ * n1 contiguous floats -- so models are [nx][nz] with z fastest and trace gathers are
+ * [ntr][ns] with time fastest.  float** arguments must point into ONE contiguous
+ * block (rows[i] == rows[0] + i*n1), as alloc2float returns.
+ */
+#ifndef FWI_B200_H
+#define FWI_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#if defined(__GNUC__)
+#define FWI_API __attribute__((visibility("default")))
+#else
+#define FWI_API
+#endif
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ------------------------------------------------------------------ status */
+enum {
+    FWI_OK = 0,
+    FWI_ERR_ARG = 1,        /* invalid argument (sizes, indices, NULL pointers) */
+    FWI_ERR_CUDA = 2,       /* a CUDA runtime call failed */
+    FWI_ERR_NOMEM = 3,      /* device or host allocation failed / over the context budget */
+    FWI_ERR_UNSUPPORTED = 4,/* a reference option this build does not implement */
+    FWI_ERR_NODEVICE = 5,   /* no CUDA device: the engine has no CPU fallback */
+    FWI_ERR_STATE = 6       /* call order (e.g. adjoint before forward) */
+};
+/* message of the last failure on the calling thread ("" if none) */
+FWI_API const char *fwi_last_error(void);
+/* library version string */
+FWI_API const char *fwi_version(void);
+
+/* ------------------------------------------------ reference types (drop-in) */
+
+/* shot record; identical layout to Record2D, observation.h:18-48 */
+typedef struct {
+    int shotID;
+    float sx, sz;
+    int isx, isz;        /* source grid index: window-local x, global z */
+    float fpeak;
+    float *src;          /* nt */
+    float *gx, *gz;      /* ntr receiver coordinates (m) */
+    int *igx, *igz;      /* ntr: window-local x, global z */
+    int sampleRate;
+    int ntr, ns;
+    float dtr, dt;
+    int ix_min, ix_max;
+    float **traces_vx, **traces_vz, **traces_p; /* traces_p: [ntr][ns] */
+    float **precond, **grad;
+} Record2D;
+
+/* wavefield checkpoint store of one shot.  Same name and life cycle as
+ * Acoustic2dCheckPoint, checkpoint.h:16-26 (init, alloc, engine mode 1 fills it,
+ * engine mode 2 consumes it, free); here the frames live in device memory. */
+typedef struct {
+    int nt, dCheckPoint, nCheckPoint, ntPoint;
+    float memCost;        /* GB the reference would hold for the same store */
+    void *impl;           /* device-side store, owned by this library */
+} Acoustic2dCheckPoint;
+
+/* replaces iso_acoustic2d_propagation, propagation.h:133-142 (propagation.c:777-1036):
+ * problem 0 forward modeling into record2d_pre[i].traces_p; problem 1 gradient into
+ * grad (and the adjoint source into record2d_pre); problem 2 forward + residual in place. */
+FWI_API void iso_acoustic2d_propagation(float **vp, float **rho, Record2D *record2d_obs, int Nshot, int nz, int nx,
+                                float dx, float dz, float dt, int nt, int pmlThick, int freesurface,
+                                float freq, float filter, int precondition, int problem, int iter,
+                                int verbose, Record2D *record2d_pre, float **grad);
+/* same contract, returns FWI_OK or an error code instead of exiting */
+FWI_API int fwi_iso_acoustic2d_propagation(float **vp, float **rho, Record2D *record2d_obs, int Nshot, int nz, int nx,
+                                   float dx, float dz, float dt, int nt, int pmlThick, int freesurface,
+                                   float freq, float filter, int precondition, int problem, int iter,
+                                   int verbose, Record2D *record2d_pre, float **grad);
+
+/* replaces iso_acoustic2d_propagation_engine, propagation.h:95-101 (propagation.c:356-775):
+ * mode 0 forward, mode 1 forward + checkpoints (+ pseudo-Hessian into grad when
+ * precondition == 1), mode 2 adjoint from the checkpoints, gradient into grad.
+ * vpm/rhom are the shot's window (nz x nx). */
+FWI_API void iso_acoustic2d_propagation_engine(Record2D *record2d, Acoustic2dCheckPoint *chkpt, float **vpm,
+                                       float **rhom, int nx, int nz, float dx, float dz, float dt, int nt,
+                                       int pmlThick, int freesurface, int precondition, int mode, int iter,
+                                       int verbose, float **grad);
+FWI_API int fwi_iso_acoustic2d_propagation_engine(Record2D *record2d, Acoustic2dCheckPoint *chkpt, float **vpm,
+                                          float **rhom, int nx, int nz, float dx, float dz, float dt, int nt,
+                                          int pmlThick, int freesurface, int precondition, int mode, int iter,
+                                          int verbose, float **grad);
+
+/* replace the checkpoint.h:27-165 life cycle (checkpoint.c:13-128, 267-298) */
+FWI_API void acoustic2dCheckPoint_init(Acoustic2dCheckPoint *chkpt);
+FWI_API void alloc_acoustic2dCheckPoint(Acoustic2dCheckPoint *chkpt, int NZ, int NX, int nt);
+FWI_API void free_acoustic2dCheckPoint(Acoustic2dCheckPoint *chkpt);
+FWI_API float calculate_memory_cost_checkpoint(int nt, int NX, int NZ);
+
+/* replace the optimization.h reductions (optimization.c:13-298), computed on the device */
+FWI_API void apply_gradient_precondition(float *grad, const float *precond, int n, float alpha);
+FWI_API void apply_gradient_shot_precondition(float *grad, float *precond, int n);
+FWI_API float calculate_objective_value(Record2D *record2d, int Nshot);
+FWI_API float calculate_step_length(Record2D *record2d_pre0, Record2D *record2d_pre1, int Nshot);
+FWI_API float compute_model_perturbation(float fraction, float *slowness, float *gradient, float *out, int len);
+/* replaces compute_adjoint_source2d, optimization.h:17-19 (optimization.c:300-419) */
+FWI_API void compute_adjoint_source2d(Record2D *record2d_pre, Record2D *record2d_obs, float **vp, float freq,
+                              int filter, Record2D *record2d_adjsource);
+/* replaces smooth2D, common.h (common.c:927-1040) */
+FWI_API void smooth2D(float **in, float **out, int nx, int nz, int N, int iszdirect);
+
+/* ------------------------------------------------------------ native API */
+
+typedef struct fwi_ctx fwi_ctx;
+
+/* one shot in flat form (the Record2D fields the engine reads) */
+typedef struct {
+    int shotID;          /* 1-based */
+    int isx, isz;        /* window-local x, global z */
+    int ntr, ns, sampleRate;
+    int ix_min, ix_max;  /* model window, inclusive */
+    float dt;            /* record sample interval */
+    float dtr;           /* receiver interval (m) */
+    float fpeak;         /* wavelet peak frequency (Hz) */
+    const float *src;    /* nt samples */
+    const int *igx;      /* ntr, window-local */
+    const int *igz;      /* ntr, global */
+} fwi_shot;
+
+/* execution paths of fwi_ctx_run */
+enum {
+    FWI_PATH_PLAIN = 0,   /* one shot per launch, one launch per time step (the straight port) */
+    FWI_PATH_BATCHED = 1  /* all shots of a batch per launch, time loop captured as CUDA graphs */
+};
+
+/* device_budget_bytes: 0 = no cap; otherwise allocations beyond it fail with FWI_ERR_NOMEM */
+FWI_API int fwi_ctx_create(fwi_ctx **ctx, int device, size_t device_budget_bytes);
+FWI_API int fwi_ctx_destroy(fwi_ctx *ctx);
+/* model on the global grid (host arrays [nx][nz]) and the run constants */
+FWI_API int fwi_ctx_set_model(fwi_ctx *ctx, const float *vp, const float *rho, int nz, int nx, float dx, float dz,
+                      float dt, int nt, int pmlThick, int freesurface);
+/* same, from device pointers (no host copy) */
+FWI_API int fwi_ctx_set_model_device(fwi_ctx *ctx, const float *d_vp, const float *d_rho, int nz, int nx, float dx,
+                             float dz, float dt, int nt, int pmlThick, int freesurface);
+FWI_API int fwi_ctx_set_shots(fwi_ctx *ctx, const fwi_shot *shots, int nshot);
+/* observed gathers: one host array [ntr][ns] per shot */
+FWI_API int fwi_ctx_set_observed(fwi_ctx *ctx, const float *const *obs);
+/* problem 0/1/2 as iso_acoustic2d_propagation; results stay on the device */
+FWI_API int fwi_ctx_run(fwi_ctx *ctx, int problem, float freq, int filter, int precondition, int path);
+/* copy results back: predicted / residual gathers of one shot, gradient [nx][nz] */
+FWI_API int fwi_ctx_get_traces(fwi_ctx *ctx, int ishot, float *out);
+FWI_API int fwi_ctx_get_gradient(fwi_ctx *ctx, float *out);
+/* device pointers of the results (valid until the next run / set call) */
+FWI_API const float *fwi_ctx_traces_device(fwi_ctx *ctx, int ishot);
+FWI_API const float *fwi_ctx_gradient_device(fwi_ctx *ctx);
+/* device-side FP64 misfit 0.5*sum(r^2) over the current residual gathers */
+FWI_API int fwi_ctx_objective(fwi_ctx *ctx, double *out);
+/* statistics of the last run */
+typedef struct {
+    double ms;               /* device time of the run (CUDA events) */
+    double cell_updates;     /* stencil applications (padded cells x steps) */
+    long long kernel_launches;
+    long long graph_launches;
+    size_t device_bytes;     /* device memory held by the context */
+} fwi_stats;
+FWI_API int fwi_ctx_stats(fwi_ctx *ctx, fwi_stats *out);
+
+#ifdef __cplusplus
+}
+#endif
+#endif
