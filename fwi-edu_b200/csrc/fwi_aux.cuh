@@ -23,7 +23,7 @@ struct GatherDesc {
 // 0: copy samples out; 1: residual + tapers (filter 2 adjoint source, optimization.c:335-418).
 // The taper multiplies the time factor first, then the trace factor (taper_traces, common.c:796-895).
 // block (32, 8): a 32x32 tile of samples x traces
-__global__ void k_gather(const GatherDesc *__restrict__ gd, int mode)
+static __global__ void k_gather(const GatherDesc *__restrict__ gd, int mode)
 {
     __shared__ float tile[32][33];
     __shared__ float tile2[32][33];
@@ -74,7 +74,7 @@ struct FinDesc {
 };
 
 // which = 0: pseudo-Hessian 4 H / (rho v)^2 (propagation.c:610-623); 1: gradient 2 G / (rho v) (:733-743)
-__global__ void k_finalize(const FinDesc *__restrict__ fd, int which)
+static __global__ void k_finalize(const FinDesc *__restrict__ fd, int which)
 {
     const FinDesc &D = fd[blockIdx.y];
     long long n = (long long)D.nxx * D.nz;
@@ -145,7 +145,7 @@ __global__ void __launch_bounds__(NT) k_sum_partial(const SumDesc *__restrict__ 
 }
 
 // sums nparts partials per descriptor in fixed order into out[2*y], out[2*y+1]
-__global__ void k_sum_final(const SumDesc *__restrict__ sd, int nparts, double *out)
+static __global__ void k_sum_final(const SumDesc *__restrict__ sd, int nparts, double *out)
 {
     const SumDesc &D = sd[blockIdx.x];
     if (threadIdx.x == 0) {
@@ -164,7 +164,7 @@ struct PrecDesc {
     long long n;
     const double *sum;  // sum of h (FP64)
 };
-__global__ void k_shot_precondition(const PrecDesc *__restrict__ pd)
+static __global__ void k_shot_precondition(const PrecDesc *__restrict__ pd)
 {
     const PrecDesc &D = pd[blockIdx.y];
     const float avg = (float)(*D.sum / (double)D.n);
@@ -182,7 +182,7 @@ struct StackShot {
     const float *g, *h;
     int ix_min, ix_max;
 };
-__global__ void k_stack(const StackShot *__restrict__ ss, int nshot, int nz, int nx, int with_h, double *gc, double *hc)
+static __global__ void k_stack(const StackShot *__restrict__ ss, int nshot, int nz, int nx, int with_h, double *gc, double *hc)
 {
     long long n = (long long)nx * nz;
     for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
@@ -201,12 +201,12 @@ __global__ void k_stack(const StackShot *__restrict__ ss, int nshot, int nz, int
 }
 
 // FP64 stacks to FP32, then global preconditioning g /= (H + alpha*rms) (optimization.c:13-56)
-__global__ void k_to_float(const double *a, float *out, long long n)
+static __global__ void k_to_float(const double *a, float *out, long long n)
 {
     for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
         out[i] = (float)a[i];
 }
-__global__ void k_global_precondition(float *grad, const float *prec, long long n, const double *sumsq, float alpha)
+static __global__ void k_global_precondition(float *grad, const float *prec, long long n, const double *sumsq, float alpha)
 {
     const float rms = (float)sqrt(*sumsq / (double)n);
     const float ar = __fmul_rn(alpha, rms);

@@ -32,6 +32,7 @@
 #include "fwi_aux.cuh"
 #include "fwi_kernels.cuh"
 #include "fwi_setup.h"
+#include "fwi_step.cuh"
 
 using namespace fwi;
 
@@ -124,6 +125,7 @@ struct fwi_ctx {
     std::map<std::string, Program> progs;
     std::map<std::string, cudaGraphExec_t> graphs;
     fwi_stats stats{};
+    int math = 0;  // 0: bit-exact arithmetic, 1: contracted multiply-adds
     long long launches = 0;
     double last_obj = 0.0;
 };
@@ -176,6 +178,7 @@ extern "C" int fwi_ctx_create(fwi_ctx **out, int device, size_t budget)
     fwi_ctx *c = new fwi_ctx();
     c->device = device;
     c->budget = budget;
+    if (const char *e = getenv("FWI_MATH")) c->math = atoi(e) ? 1 : 0;
     CK(cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking));
     CK(cudaEventCreate(&c->ev0));
     CK(cudaEventCreate(&c->ev1));
@@ -426,6 +429,7 @@ static int prepare_run(fwi_ctx *c, ShotRun *r, int shot, bool gradient)
         TRY(ralloc(c, r, &q, (size_t)(d.Nx + 1) * 4)); d.colptr = (int *)q;
         TRY(ralloc(c, r, &q, (size_t)ntr * 8)); d.rec = (int2 *)q;
         TRY(ralloc(c, r, &q, (size_t)ntr * 4)); d.recK = (float *)q;
+        TRY(ralloc(c, r, &q, (size_t)ntr * 4)); d.rec_off = (int *)q;
         TRY(ralloc(c, r, &q, (size_t)s.ns * ntr * 4)); d.traces_t = (float *)q;
         TRY(ralloc(c, r, &q, 3 * fr * 4)); d.fscr = (float *)q;
         d.ckslots = d.rscr = d.seg = d.ascr = nullptr;
@@ -470,6 +474,8 @@ static int prepare_run(fwi_ctx *c, ShotRun *r, int shot, bool gradient)
     std::vector<int> colptr(d.Nx + 1, 0);
     std::vector<int2> rec(ntr);
     std::vector<float> recK(ntr);
+    std::vector<int> rec_off(ntr);
+    for (int i = 0; i < ntr; i++) rec_off[i] = (sh.igx[i] + c->pml) * d.ld + sh.igz[i] + c->pml;
     for (int e = 0; e < ntr; e++) {
         int i = order[e];
         int X = sh.igx[i] + c->pml, Z = sh.igz[i] + c->pml;
@@ -483,6 +489,7 @@ static int prepare_run(fwi_ctx *c, ShotRun *r, int shot, bool gradient)
     CK(cudaMemcpyAsync((void *)d.colptr, colptr.data(), (d.Nx + 1) * 4, cudaMemcpyHostToDevice, c->stream));
     CK(cudaMemcpyAsync((void *)d.rec, rec.data(), ntr * 8, cudaMemcpyHostToDevice, c->stream));
     CK(cudaMemcpyAsync((void *)d.recK, recK.data(), ntr * 4, cudaMemcpyHostToDevice, c->stream));
+    CK(cudaMemcpyAsync((void *)d.rec_off, rec_off.data(), ntr * 4, cudaMemcpyHostToDevice, c->stream));
     CK(cudaStreamSynchronize(c->stream));  // host staging vectors go out of scope
     return FWI_OK;
 }
@@ -597,40 +604,54 @@ static int get_program(fwi_ctx *c, const std::string &key, const std::vector<int
 // ---------------------------------------------------------------- launching
 typedef void (*StepFn)(const ShotDesc *, const int4 *, int, int, int);
 
-static void pick_launch(int Nx, int nshot, bool batched, int *lx, StepFn *fn)
+template <int S, int MATH>
+static StepFn step_fn(int tx)
 {
-    // blocks = strips x shots x 2; the single-shot path wants many small strips
-    int want = batched ? 32 : 8;
-    if (!batched && Nx / want < 2 * 148) want = 4;
-    (void)nshot;
-    *lx = want;
-    switch (want) {
-    case 4: *fn = k_step<4>; break;
-    case 8: *fn = k_step<8>; break;
-    case 16: *fn = k_step<16>; break;
-    default: *fn = k_step<32>; break;
+    StepFn f;
+    switch (tx) {
+    case 8: f = k_step<8, S, MATH>; break;
+    default: f = k_step<16, S, MATH>; break;
     }
+    // the tiles live in shared memory: prefer the largest carve-out so more blocks fit per SM
+    cudaFuncSetAttribute((const void *)f, cudaFuncAttributePreferredSharedMemoryCarveout,
+                         cudaSharedmemCarveoutMaxShared);
+    return f;
+}
+
+// launch shape: tiles of 16 z-groups x TX columns, S shots per block sharing one coefficient load
+struct LaunchCfg {
+    int tx, S, math;
+    StepFn fn;
+};
+static LaunchCfg pick_launch(int Nx, int nshot, bool batched, int math)
+{
+    LaunchCfg L;
+    L.tx = batched ? 16 : 8;
+    L.S = (batched && nshot >= 2) ? 2 : 1;
+    L.math = math;
+    (void)Nx;
+    if (const char *e = getenv("FWI_TX")) L.tx = atoi(e);
+    if (const char *e = getenv("FWI_S")) L.S = atoi(e);
+    if (L.tx != 8) L.tx = 16;
+    if (L.S != 1) L.S = 2;
+    if (L.S == 1) L.fn = L.math ? step_fn<1, 1>(L.tx) : step_fn<1, 0>(L.tx);
+    else L.fn = L.math ? step_fn<2, 1>(L.tx) : step_fn<2, 0>(L.tx);
+    return L;
 }
 
 static int launch_steps(fwi_ctx *c, const Program *prog, int shot_base, int nshot, int prog_stride, const Plan *p,
                         bool batched)
 {
-    int lx;
-    StepFn fn;
-    pick_launch(p->Nx, nshot, batched, &lx, &fn);
-    const int W = (p->G + 31) / 32;
-    int threads = 32 * W, zchunks = 1;
-    if (threads > 256) {  // very tall columns: split the column over several blocks
-        zchunks = (threads + 255) / 256;
-        threads = 256;
-    }
-    if (zchunks > 1) return fail(FWI_ERR_UNSUPPORTED, "grid with %d padded rows is taller than one block", p->Nz);
-    dim3 grid((p->Nx + lx - 1) / lx, 2 * nshot, zchunks);
+    (void)prog_stride;
+    LaunchCfg cfg = pick_launch(p->Nx, nshot, batched, c->math);
+    const int zt = (p->G + TG - 1) / TG;
+    const int groups = (nshot + cfg.S - 1) / cfg.S;
+    dim3 grid((p->Nx + cfg.tx - 1) / cfg.tx + 1, 2 * groups, zt);
     const int n = (int)prog->items.size();
     for (int L = 0; L < n; L++) {
         const int4 &pw = prog->items[L];
         if (pw.x == K_NONE && pw.z == K_NONE) continue;
-        fn<<<grid, threads, 0, c->stream>>>(c->d_desc, prog->d, prog_stride, L, shot_base);
+        cfg.fn<<<grid, dim3(TG, TYX), 0, c->stream>>>(c->d_desc, prog->d, L, shot_base, nshot);
         c->launches++;
     }
     CK(cudaGetLastError());
@@ -875,6 +896,8 @@ static int run_program(fwi_ctx *c, const std::string &key, const Program *prog, 
                        const Plan *p, bool batched)
 {
     if (!batched) return launch_steps(c, prog, shot_base, nshot, 0, p, false);
+    const char *ge = getenv("FWI_GRAPH");  // FWI_GRAPH=0: issue the launches directly (profilers, debugging)
+    if (ge && ge[0] == '0') return launch_steps(c, prog, shot_base, nshot, 0, p, true);
     auto it = c->graphs.find(key);
     if (it == c->graphs.end()) {
         cudaGraph_t g;
@@ -914,24 +937,40 @@ static int run_forward_group(fwi_ctx *c, std::vector<ShotRun *> &rs, int problem
     return FWI_OK;
 }
 
+// forward pass of a gradient (engine mode 1): checkpoints, samples, pseudo-Hessian
+static int grad_forward(fwi_ctx *c, std::vector<ShotRun *> &rs, int precondition, bool batched,
+                        const std::string &gkey, int shot_base)
+{
+    Program *pf;
+    TRY(get_program(c, "fwd1", program_forward(c->nt, K_FWD1), &pf));
+    for (ShotRun *r : rs) TRY(zero_initial(c, r, true));
+    TRY(run_program(c, "fwd1/" + gkey, pf, shot_base, (int)rs.size(), rs[0]->plan, batched));
+    if (precondition == 1) TRY(finalize(c, rs, 0));
+    return FWI_OK;
+}
+
+// adjoint pass (engine mode 2) from the adjoint sources in adj_t: replay + adjoint + imaging
+static int grad_adjoint(fwi_ctx *c, std::vector<ShotRun *> &rs, bool batched, const std::string &gkey, int shot_base)
+{
+    Program *pa;
+    TRY(get_program(c, batched ? "adj/overlap" : "adj/plain", program_adjoint(c->nt, batched), &pa));
+    TRY(adj_init(c, rs, shot_base));
+    TRY(run_program(c, std::string(batched ? "adjo/" : "adjp/") + gkey, pa, shot_base, (int)rs.size(), rs[0]->plan,
+                    batched));
+    TRY(finalize(c, rs, 1));
+    return FWI_OK;
+}
+
 static int run_gradient_group(fwi_ctx *c, std::vector<ShotRun *> &rs, float freq, int filter, int precondition,
                               bool batched, const std::string &gkey, int shot_base)
 {
     if (filter == 0 || filter == 1) return fail(FWI_ERR_UNSUPPORTED, "residual filter %d (FFT) is not built", filter);
     for (ShotRun *r : rs)
         if (r->d.sr > 1) return fail(FWI_ERR_UNSUPPORTED, "sampleRate > 1 needs FFT trace interpolation (not built)");
-    Program *pf, *pa;
-    TRY(get_program(c, "fwd1", program_forward(c->nt, K_FWD1), &pf));
-    TRY(get_program(c, batched ? "adj/overlap" : "adj/plain", program_adjoint(c->nt, batched), &pa));
-    for (ShotRun *r : rs) TRY(zero_initial(c, r, true));
-    TRY(run_program(c, "fwd1/" + gkey, pf, shot_base, (int)rs.size(), rs[0]->plan, batched));
-    if (precondition == 1) TRY(finalize(c, rs, 0));
+    TRY(grad_forward(c, rs, precondition, batched, gkey, shot_base));
     for (ShotRun *r : rs) TRY(prepare_taper(c, r, freq));
     TRY(gather(c, rs, 1, true));
-    TRY(adj_init(c, rs, shot_base));
-    TRY(run_program(c, std::string(batched ? "adjo/" : "adjp/") + gkey, pa, shot_base, (int)rs.size(), rs[0]->plan,
-                    batched));
-    TRY(finalize(c, rs, 1));
+    TRY(grad_adjoint(c, rs, batched, gkey, shot_base));
     if (precondition == 1) TRY(shot_precondition(c, rs));
     return FWI_OK;
 }
@@ -1085,9 +1124,158 @@ extern "C" int fwi_ctx_objective(fwi_ctx *c, double *out)
     return FWI_OK;
 }
 
+extern "C" int fwi_adjoint_program(int nt, int overlap, int *items, int cap)
+{
+    if (nt <= 0) return 0;
+    std::vector<int4> p = program_adjoint(nt, overlap != 0);
+    if (items)
+        for (int i = 0; i < (int)p.size() && i < cap; i++) {
+            items[4 * i] = p[i].x;
+            items[4 * i + 1] = p[i].y;
+            items[4 * i + 2] = p[i].z;
+            items[4 * i + 3] = p[i].w;
+        }
+    return (int)p.size();
+}
+
+extern "C" int fwi_checkpoint_interval(int nt) { return fwi_ck_interval(nt); }
+
 extern "C" int fwi_ctx_stats(fwi_ctx *c, fwi_stats *out)
 {
     if (!c || !out) return fail(FWI_ERR_ARG, "NULL argument");
     *out = c->stats;
     return FWI_OK;
+}
+
+// ------------------------------------------------------------------ engine drop-in
+// iso_acoustic2d_propagation_engine with the reference's checkpoint object: mode 1 runs
+// the forward pass into a context owned by the checkpoint object (its frames stay on
+// the device), mode 2 runs the adjoint pass from them.  Mode 0 uses a shared context.
+namespace {
+struct CkImpl {
+    fwi_ctx *ctx = nullptr;
+    bool forward_done = false;
+};
+fwi_ctx *g_engine_ctx = nullptr;
+
+bool rows_contiguous(float **rows, int n1, int n2)
+{
+    for (int i = 1; i < n2; i++)
+        if (rows[i] != rows[0] + (size_t)i * n1) return false;
+    return true;
+}
+}  // namespace
+
+// [ntr][ns] host adjoint source -> adj_t [nt][ntr] on the device (interpolate_traces with r = 1 is a copy)
+static __global__ void k_to_time_major(const float *__restrict__ a, float *__restrict__ out, int ntr, int ns, int nt)
+{
+    long long n = (long long)ntr * nt;
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+        int k = (int)(i / ntr), r = (int)(i % ntr);
+        out[i] = k < ns ? a[(long long)r * ns + k] : 0.0f;
+    }
+}
+
+extern "C" void acoustic2dCheckPoint_init(Acoustic2dCheckPoint *chk)
+{
+    if (chk) memset(chk, 0, sizeof(*chk));
+}
+
+extern "C" void alloc_acoustic2dCheckPoint(Acoustic2dCheckPoint *chk, int NZ, int NX, int nt)
+{
+    if (!chk) return;
+    free_acoustic2dCheckPoint(chk);
+    chk->nt = nt;
+    chk->dCheckPoint = fwi_ck_interval(nt);
+    chk->nCheckPoint = fwi_ck_count(nt);
+    chk->ntPoint = chk->nCheckPoint + chk->dCheckPoint - 2;
+    chk->memCost = 1.0f * (chk->ntPoint * NZ * NX * (int)sizeof(float)) / powf(1024.0f, 3);
+    chk->impl = new CkImpl();
+}
+
+extern "C" void free_acoustic2dCheckPoint(Acoustic2dCheckPoint *chk)
+{
+    if (!chk || !chk->impl) return;
+    CkImpl *k = (CkImpl *)chk->impl;
+    if (k->ctx) fwi_ctx_destroy(k->ctx);
+    delete k;
+    chk->impl = nullptr;
+}
+
+extern "C" int fwi_iso_acoustic2d_propagation_engine(Record2D *r, Acoustic2dCheckPoint *chk, float **vpm, float **rhom,
+                                                     int nx, int nz, float dx, float dz, float dt, int nt, int pml,
+                                                     int fs, int precondition, int mode, int iter, int verbose,
+                                                     float **grad)
+{
+    (void)iter;
+    (void)verbose;
+    if (!r || !vpm || !rhom || mode < 0 || mode > 2) return fail(FWI_ERR_ARG, "invalid engine arguments");
+    if (!rows_contiguous(vpm, nz, nx) || !rows_contiguous(rhom, nz, nx))
+        return fail(FWI_ERR_ARG, "vpm/rhom must be one contiguous block (alloc2float layout)");
+    if (mode > 0 && (!chk || !chk->impl)) return fail(FWI_ERR_STATE, "modes 1 and 2 need an allocated checkpoint");
+    if (mode == 2 && !grad) return fail(FWI_ERR_ARG, "mode 2 writes the gradient: grad is NULL");
+    fwi_ctx *c;
+    CkImpl *k = mode > 0 ? (CkImpl *)chk->impl : nullptr;
+    if (mode == 0) {
+        if (!g_engine_ctx) TRY(fwi_ctx_create(&g_engine_ctx, 0, 0));
+        c = g_engine_ctx;
+    } else {
+        if (!k->ctx) TRY(fwi_ctx_create(&k->ctx, 0, 0));
+        c = k->ctx;
+    }
+    fwi_shot s{};
+    s.shotID = r->shotID; s.isx = r->isx; s.isz = r->isz; s.ntr = r->ntr; s.ns = r->ns;
+    s.sampleRate = r->sampleRate; s.ix_min = 0; s.ix_max = nx - 1;  // vpm is the shot's window already
+    s.dt = r->dt; s.dtr = r->dtr; s.fpeak = r->fpeak;
+    s.src = r->src; s.igx = r->igx; s.igz = r->igz;
+    if (mode == 2) {
+        if (!k->forward_done) return fail(FWI_ERR_STATE, "mode 2 before mode 1 on this checkpoint");
+        if (r->sampleRate > 1) return fail(FWI_ERR_UNSUPPORTED, "sampleRate > 1 needs FFT trace interpolation (not built)");
+        CK(cudaSetDevice(c->device));
+        ShotRun *sr = c->runs[0].get();
+        const size_t nb = (size_t)r->ntr * r->ns * 4;
+        CK(cudaMemcpyAsync(c->d_pre[0], r->traces_p[0], nb, cudaMemcpyHostToDevice, c->stream));
+        k_to_time_major<<<296, 256, 0, c->stream>>>(c->d_pre[0], (float *)sr->d.adj_t, r->ntr, r->ns, nt);
+        CK(cudaGetLastError());
+        std::vector<ShotRun *> rs = {sr};
+        TRY(grad_adjoint(c, rs, false, "", 0));
+        CK(cudaMemcpyAsync(grad[0], sr->d_gshot, (size_t)nx * nz * 4, cudaMemcpyDeviceToHost, c->stream));
+        CK(cudaStreamSynchronize(c->stream));
+        return FWI_OK;
+    }
+    TRY(fwi_ctx_set_model(c, vpm[0], rhom[0], nz, nx, dx, dz, dt, nt, pml, fs));
+    TRY(fwi_ctx_set_shots(c, &s, 1));
+    if (mode == 0) {
+        TRY(fwi_ctx_run(c, 0, 0.0f, 2, 0, FWI_PATH_PLAIN));
+        return fwi_ctx_get_traces(c, 0, r->traces_p[0]);
+    }
+    // mode 1
+    CK(cudaSetDevice(c->device));
+    if (c->runs.size() != 1) {
+        free_runs(c);
+        c->runs.emplace_back(new ShotRun());
+    }
+    ShotRun *sr = c->runs[0].get();
+    TRY(prepare_run(c, sr, 0, true));
+    sr->d.hessian = precondition == 1;
+    TRY(upload_descs(c, {sr->d}));
+    std::vector<ShotRun *> rs = {sr};
+    TRY(grad_forward(c, rs, precondition, false, "", 0));
+    TRY(gather(c, rs, 0, false));
+    TRY(fwi_ctx_get_traces(c, 0, r->traces_p[0]));
+    if (precondition == 1 && grad)
+        CK(cudaMemcpyAsync(grad[0], sr->d_hshot, (size_t)nx * nz * 4, cudaMemcpyDeviceToHost, c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+    k->forward_done = true;
+    return FWI_OK;
+}
+
+extern "C" void iso_acoustic2d_propagation_engine(Record2D *r, Acoustic2dCheckPoint *chk, float **vpm, float **rhom,
+                                                  int nx, int nz, float dx, float dz, float dt, int nt, int pml, int fs,
+                                                  int precondition, int mode, int iter, int verbose, float **grad)
+{
+    int rc = fwi_iso_acoustic2d_propagation_engine(r, chk, vpm, rhom, nx, nz, dx, dz, dt, nt, pml, fs, precondition, mode,
+                                                   iter, verbose, grad);
+    if (rc != FWI_OK)
+        fprintf(stderr, "<error>: iso_acoustic2d_propagation_engine failed (status %d): %s\n", rc, g_err.c_str());
 }

@@ -1,7 +1,259 @@
-// fwi_ops.cu -- checkpoint-store bookkeeping of the reference interface.
+// fwi_ops.cu -- the reference-named FWI-loop operations (optimization.c, common.c),
+// computed on the device.  These keep the reference's host-array interfaces so a
+// front-end written against FWI-EDU links unchanged; each call stages its arrays
+// through one process-wide device workspace.  The device-resident FWI iteration of
+// fwi_engine.cu runs the same kernels without the host round trips.
+#include <cuda_runtime.h>
+
 #include <cmath>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <mutex>
+#include <vector>
+
 #include "../../include/fwi_b200.h"
+#include "fwi_aux.cuh"
+#include "fwi_optim.cuh"
 #include "fwi_setup.h"
+
+using namespace fwi;
+
+namespace {
+
+struct Ops {
+    int dev = -1;
+    cudaStream_t st = nullptr;
+    char *buf = nullptr;
+    size_t cap = 0;
+};
+Ops g_ops;
+std::mutex g_ops_mu;
+
+bool report(cudaError_t e, const char *what)
+{
+    if (e == cudaSuccess) return true;
+    fprintf(stderr, "<error>: %s: %s\n", what, cudaGetErrorString(e));
+    return false;
+}
+
+// workspace of at least `bytes`, 256-byte aligned sub-buffers handed out by offset
+bool ops_ready(size_t bytes)
+{
+    int dev = 0;
+    if (const char *p = getenv("FWI_DEVICE")) dev = atoi(p);
+    if (g_ops.dev != dev) {
+        int n = 0;
+        if (cudaGetDeviceCount(&n) != cudaSuccess || n <= dev) {
+            fprintf(stderr, "<error>: no CUDA device %d: the FWI operations run on the GPU only\n", dev);
+            return false;
+        }
+        if (!report(cudaSetDevice(dev), "cudaSetDevice")) return false;
+        if (!report(cudaStreamCreateWithFlags(&g_ops.st, cudaStreamNonBlocking), "cudaStreamCreate")) return false;
+        g_ops.dev = dev;
+    }
+    if (!report(cudaSetDevice(dev), "cudaSetDevice")) return false;
+    if (bytes > g_ops.cap) {
+        if (g_ops.buf) cudaFree(g_ops.buf);
+        g_ops.buf = nullptr;
+        g_ops.cap = 0;
+        if (!report(cudaMalloc(&g_ops.buf, bytes), "cudaMalloc")) return false;
+        g_ops.cap = bytes;
+    }
+    return true;
+}
+
+size_t al(size_t b) { return (b + 255) & ~size_t(255); }
+
+// FP64 sums of one or two operand arrays already on the device
+bool dsum(const float *a, const float *b, long long n, int op, double out[2])
+{
+    const int NP = 592;
+    char *base = g_ops.buf + g_ops.cap - al(sizeof(SumDesc)) - al(2 * NP * 8 + 16);
+    SumDesc h{};
+    h.a = a;
+    h.b = b;
+    h.n = n;
+    h.op = op;
+    h.partial = (double *)(base + al(sizeof(SumDesc)));
+    double *res = h.partial + 2 * NP;
+    if (!report(cudaMemcpyAsync(base, &h, sizeof(h), cudaMemcpyHostToDevice, g_ops.st), "copy")) return false;
+    k_sum_partial<256><<<dim3(NP, 1), 256, 0, g_ops.st>>>((const SumDesc *)base);
+    k_sum_final<<<1, 32, 0, g_ops.st>>>((const SumDesc *)base, NP, res);
+    if (!report(cudaMemcpyAsync(out, res, 16, cudaMemcpyDeviceToHost, g_ops.st), "copy")) return false;
+    return report(cudaStreamSynchronize(g_ops.st), "reduction");
+}
+const size_t RED_BYTES = 2 * 592 * 8 + 4096;
+
+}  // namespace
+
+// calculate_objective_value, optimization.c:99-132: 0.5 * sum over shots of traces^2 (FP64)
+extern "C" float calculate_objective_value(Record2D *r, int Nshot)
+{
+    std::lock_guard<std::mutex> lk(g_ops_mu);
+    long long n = 0;
+    for (int i = 0; i < Nshot; i++) n += (long long)r[i].ntr * r[i].ns;
+    if (!ops_ready(al(n * 4) + RED_BYTES)) return NAN;
+    float *d = (float *)g_ops.buf;
+    long long off = 0;
+    for (int i = 0; i < Nshot; i++) {
+        size_t b = (size_t)r[i].ntr * r[i].ns * 4;
+        if (!report(cudaMemcpyAsync(d + off, r[i].traces_p[0], b, cudaMemcpyHostToDevice, g_ops.st), "copy")) return NAN;
+        off += (long long)r[i].ntr * r[i].ns;
+    }
+    double s[2];
+    if (!dsum(d, nullptr, n, 1, s)) return NAN;
+    return (float)(0.5 * s[0]);
+}
+
+// calculate_step_length, optimization.c:134-176: sum r0 (r0 - r1) / sum (r0 - r1)^2
+extern "C" float calculate_step_length(Record2D *p0, Record2D *p1, int Nshot)
+{
+    std::lock_guard<std::mutex> lk(g_ops_mu);
+    long long n = 0;
+    for (int i = 0; i < Nshot; i++) n += (long long)p0[i].ntr * p0[i].ns;
+    if (!ops_ready(2 * al(n * 4) + RED_BYTES)) return NAN;
+    float *a = (float *)g_ops.buf, *b = (float *)(g_ops.buf + al(n * 4));
+    long long off = 0;
+    for (int i = 0; i < Nshot; i++) {
+        size_t nb = (size_t)p0[i].ntr * p0[i].ns * 4;
+        cudaMemcpyAsync(a + off, p0[i].traces_p[0], nb, cudaMemcpyHostToDevice, g_ops.st);
+        cudaMemcpyAsync(b + off, p1[i].traces_p[0], nb, cudaMemcpyHostToDevice, g_ops.st);
+        off += (long long)p0[i].ntr * p0[i].ns;
+    }
+    double s[2];
+    if (!dsum(a, b, n, 3, s)) return NAN;
+    if (s[1] == 0.0) {
+        fprintf(stderr, "<warning>: denominator is zero in step length calculation, returning 0.\n");
+        return 0.0f;
+    }
+    return (float)(s[0] / s[1]);
+}
+
+// compute_model_perturbation, optimization.c:178-298
+extern "C" float compute_model_perturbation(float fraction, float *slowness, float *gradient, float *out, int len)
+{
+    std::lock_guard<std::mutex> lk(g_ops_mu);
+    if (len <= 0) return 0.0f;
+    size_t nb = al((size_t)len * 4);
+    if (!ops_ready(3 * nb + al(sizeof(PertState)) + RED_BYTES)) return NAN;
+    float *g = (float *)g_ops.buf, *sl = (float *)(g_ops.buf + nb), *o = (float *)(g_ops.buf + 2 * nb);
+    PertState *st = (PertState *)(g_ops.buf + 3 * nb);
+    cudaMemcpyAsync(g, gradient, (size_t)len * 4, cudaMemcpyHostToDevice, g_ops.st);
+    cudaMemcpyAsync(sl, slowness, (size_t)len * 4, cudaMemcpyHostToDevice, g_ops.st);
+    double s[2];
+    if (!dsum(sl, nullptr, len, 0, s)) return NAN;
+    double *ssum = (double *)((char *)st + offsetof(PertState, avg_slow));
+    k_pert_init<<<1, 256, 0, g_ops.st>>>(st);
+    cudaMemcpyAsync(ssum, &s[0], 8, cudaMemcpyHostToDevice, g_ops.st);
+    k_pert_minmax<<<296, 256, 0, g_ops.st>>>(g, len, st);
+    k_pert_hist<<<296, 256, 0, g_ops.st>>>(g, len, st);
+    k_pert_scalar<<<1, 32, 0, g_ops.st>>>(st, ssum, len, fraction);
+    k_pert_apply<<<296, 256, 0, g_ops.st>>>(g, o, len, st);
+    float scalar = NAN;
+    cudaMemcpyAsync(&scalar, (char *)st + offsetof(PertState, scalar), 4, cudaMemcpyDeviceToHost, g_ops.st);
+    cudaMemcpyAsync(out, o, (size_t)len * 4, cudaMemcpyDeviceToHost, g_ops.st);
+    if (!report(cudaStreamSynchronize(g_ops.st), "compute_model_perturbation")) return NAN;
+    return scalar;
+}
+
+// smooth2D, common.c:927-1040: one cos^2 pass along z (iszdirect == 1) or x
+extern "C" void smooth2D(float **in, float **out, int nx, int nz, int N, int iszdirect)
+{
+    std::lock_guard<std::mutex> lk(g_ops_mu);
+    size_t m = (size_t)nx * nz;
+    size_t nb = al(m * 4);
+    if (!ops_ready(2 * nb + al((2 * N + 1) * 4))) return;
+    std::vector<float> w(2 * N + 1);
+    for (int i = 0; i < 2 * N + 1; i++) {
+        w[i] = (float)cos(3.141592653589793 * (i - N) / (2.0 * N));
+        w[i] *= w[i];
+    }
+    float *a = (float *)g_ops.buf, *b = (float *)(g_ops.buf + nb), *dw = (float *)(g_ops.buf + 2 * nb);
+    cudaMemcpyAsync(a, in[0], m * 4, cudaMemcpyHostToDevice, g_ops.st);
+    cudaMemcpyAsync(dw, w.data(), w.size() * 4, cudaMemcpyHostToDevice, g_ops.st);
+    k_smooth2d<<<592, 256, 0, g_ops.st>>>(a, b, nx, nz, N, iszdirect == 1, dw);
+    cudaMemcpyAsync(out[0], b, m * 4, cudaMemcpyDeviceToHost, g_ops.st);
+    report(cudaStreamSynchronize(g_ops.st), "smooth2D");
+}
+
+// compute_adjoint_source2d, optimization.c:300-419 (filter 2: residual and tapers)
+extern "C" void compute_adjoint_source2d(Record2D *pre, Record2D *obs, float **vp, float freq, int filter,
+                                         Record2D *adj)
+{
+    std::lock_guard<std::mutex> lk(g_ops_mu);
+    if (filter == 0 || filter == 1) {
+        fprintf(stderr, "<error>: compute_adjoint_source2d: residual filter %d (FFT) is not built\n", filter);
+        return;
+    }
+    const int ns = adj->ns, ntr = adj->ntr;
+    double vp_sum = 0.0;
+    for (int i = 0; i < ntr; i++) vp_sum += vp[adj->igx[i]][adj->igz[i]];  // window-local igx, global vp
+    float vp_avg = (float)(vp_sum / ntr);
+    if (freq == 0.0f) freq = adj->fpeak;
+    float kpass = freq / vp_avg;
+    int Lt = (int)roundf((2.0f / freq) / adj->dt) + 1;
+    int Lr = (int)roundf((2.0f / kpass) / adj->dtr) + 1;
+    if (Lt > 0 && Lt > ns / 3) Lt = ns / 3;
+    if (Lr > 0 && Lr > ntr / 3) Lr = ntr / 3;
+    if (Lt < 0) Lt = 0;
+    if (Lr < 0) Lr = 0;
+    std::vector<float> tct(Lt + 1), tcr(Lr + 1);
+    if (Lt > 0) fwi_taper_coefs(Lt, tct.data());
+    if (Lr > 0) fwi_taper_coefs(Lr, tcr.data());
+    size_t m = (size_t)ns * ntr, nb = al(m * 4);
+    if (!ops_ready(3 * nb + al((Lt + 1) * 4) + al((Lr + 1) * 4))) return;
+    float *dp = (float *)g_ops.buf, *dob = (float *)(g_ops.buf + nb), *da = (float *)(g_ops.buf + 2 * nb);
+    float *dt_ = (float *)(g_ops.buf + 3 * nb), *dr = (float *)(g_ops.buf + 3 * nb + al((Lt + 1) * 4));
+    cudaMemcpyAsync(dp, pre->traces_p[0], m * 4, cudaMemcpyHostToDevice, g_ops.st);
+    cudaMemcpyAsync(dob, obs->traces_p[0], m * 4, cudaMemcpyHostToDevice, g_ops.st);
+    cudaMemcpyAsync(dt_, tct.data(), (Lt + 1) * 4, cudaMemcpyHostToDevice, g_ops.st);
+    cudaMemcpyAsync(dr, tcr.data(), (Lr + 1) * 4, cudaMemcpyHostToDevice, g_ops.st);
+    k_residual_taper<<<296, 256, 0, g_ops.st>>>(dp, dob, da, ns, ntr, Lt, Lr, dt_, dr);
+    cudaMemcpyAsync(adj->traces_p[0], da, m * 4, cudaMemcpyDeviceToHost, g_ops.st);
+    report(cudaStreamSynchronize(g_ops.st), "compute_adjoint_source2d");
+}
+
+// apply_gradient_shot_precondition, optimization.c:58-97
+extern "C" void apply_gradient_shot_precondition(float *grad, float *precond, int n)
+{
+    std::lock_guard<std::mutex> lk(g_ops_mu);
+    size_t nb = al((size_t)n * 4);
+    if (!ops_ready(2 * nb + al(sizeof(PrecDesc)) + 256 + RED_BYTES)) return;
+    float *g = (float *)g_ops.buf, *h = (float *)(g_ops.buf + nb);
+    PrecDesc *pd = (PrecDesc *)(g_ops.buf + 2 * nb);
+    double *sum = (double *)(g_ops.buf + 2 * nb + al(sizeof(PrecDesc)));
+    cudaMemcpyAsync(g, grad, (size_t)n * 4, cudaMemcpyHostToDevice, g_ops.st);
+    cudaMemcpyAsync(h, precond, (size_t)n * 4, cudaMemcpyHostToDevice, g_ops.st);
+    double s[2];
+    if (!dsum(h, nullptr, n, 0, s)) return;
+    PrecDesc p{g, h, n, sum};
+    cudaMemcpyAsync(sum, &s[0], 8, cudaMemcpyHostToDevice, g_ops.st);
+    cudaMemcpyAsync(pd, &p, sizeof(p), cudaMemcpyHostToDevice, g_ops.st);
+    k_shot_precondition<<<dim3(148, 1), 256, 0, g_ops.st>>>(pd);
+    cudaMemcpyAsync(grad, g, (size_t)n * 4, cudaMemcpyDeviceToHost, g_ops.st);
+    cudaMemcpyAsync(precond, h, (size_t)n * 4, cudaMemcpyDeviceToHost, g_ops.st);
+    report(cudaStreamSynchronize(g_ops.st), "apply_gradient_shot_precondition");
+}
+
+// apply_gradient_precondition, optimization.c:13-56: g /= (H + alpha * rms(H))
+extern "C" void apply_gradient_precondition(float *grad, const float *precond, int n, float alpha)
+{
+    std::lock_guard<std::mutex> lk(g_ops_mu);
+    if (alpha <= 0.0f) alpha = 0.005f;
+    size_t nb = al((size_t)n * 4);
+    if (!ops_ready(2 * nb + 256 + RED_BYTES)) return;
+    float *g = (float *)g_ops.buf, *h = (float *)(g_ops.buf + nb);
+    double *sum = (double *)(g_ops.buf + 2 * nb);
+    cudaMemcpyAsync(g, grad, (size_t)n * 4, cudaMemcpyHostToDevice, g_ops.st);
+    cudaMemcpyAsync(h, precond, (size_t)n * 4, cudaMemcpyHostToDevice, g_ops.st);
+    double s[2];
+    if (!dsum(h, nullptr, n, 2, s)) return;
+    cudaMemcpyAsync(sum, &s[0], 8, cudaMemcpyHostToDevice, g_ops.st);
+    k_global_precondition<<<296, 256, 0, g_ops.st>>>(g, h, n, sum, alpha);
+    cudaMemcpyAsync(grad, g, (size_t)n * 4, cudaMemcpyDeviceToHost, g_ops.st);
+    report(cudaStreamSynchronize(g_ops.st), "apply_gradient_precondition");
+}
 
 // calculate_memory_cost_checkpoint, checkpoint.c:267-298: GB of the (nCheckPoint + d - 2)-frame store
 extern "C" float calculate_memory_cost_checkpoint(int nt, int NX, int NZ)

@@ -233,3 +233,57 @@ int fwi_setup_coefs(const float *vpm, const float *rhom, int nz, int nxx, int pm
     free(vp); free(rho); free(Dx); free(Dz); free(Bx); free(Bz); free(K); free(ir); free(irx); free(irz);
     return 0;
 }
+
+/* set_waterlayer_value, clip_model, v2slow/slow2v, vp2density (common.c:218-330, 898-924) */
+static void water_layer(float *m, float v, int wd, int nx, int nz)
+{
+    for (int ix = 0; ix < nx; ix++)
+        for (int iz = 0; iz < wd; iz++) m[(size_t)ix * nz + iz] = v;
+}
+static void clip(float *m, size_t n, float lo, float hi)
+{
+    for (size_t i = 0; i < n; i++) {
+        if (m[i] > hi) m[i] = hi;
+        else if (m[i] < lo) m[i] = lo;
+    }
+}
+static void reciprocal(const float *a, float *b, size_t n)
+{
+    for (size_t i = 0; i < n; i++) b[i] = a[i] != 0.0f ? 1.0f / a[i] : 0.0f;
+}
+static void gardner(const float *vp, float *rho, size_t n)
+{
+    for (size_t i = 0; i < n; i++) rho[i] = 310.0f * powf(vp[i], 0.25f);
+}
+
+void fwi_model_trial(const float *slow, const float *perturb, float *vp, float *rho, int nx, int nz, int waterdepth,
+                     float vp_water, float rho_water, float vpmin, float vpmax, float rhomin, float rhomax, int g)
+{
+    size_t n = (size_t)nx * nz;
+    for (size_t i = 0; i < n; i++) vp[i] = slow[i] + perturb[i];
+    reciprocal(vp, vp, n);
+    water_layer(vp, vp_water, waterdepth, nx, nz);
+    clip(vp, n, vpmin, vpmax);
+    if (g == 1) {
+        gardner(vp, rho, n);
+        water_layer(rho, rho_water, waterdepth, nx, nz);
+        clip(rho, n, rhomin, rhomax);
+    }
+}
+
+void fwi_model_update(float *slow, float *vp, float *rho, const float *perturb, float steplen, int nx, int nz,
+                      int waterdepth, float vp_water, float rho_water, float vpmin, float vpmax, float rhomin,
+                      float rhomax, int g)
+{
+    size_t n = (size_t)nx * nz;
+    for (size_t i = 0; i < n; i++) slow[i] = slow[i] + steplen * perturb[i];
+    reciprocal(slow, vp, n);
+    water_layer(vp, vp_water, waterdepth, nx, nz);
+    clip(vp, n, vpmin, vpmax);
+    if (g == 1) {
+        gardner(vp, rho, n);
+        water_layer(rho, rho_water, waterdepth, nx, nz);
+        clip(rho, n, rhomin, rhomax);
+    }
+    reciprocal(vp, slow, n);
+}

@@ -31,6 +31,14 @@ int fwi_ck_count(int nt);
 double fwi_src_term_f64(float src, float K, float dt, float invdx, float invdz);
 /* replay source / adjoint injection scale src*K*dt*dt*invdx*invdz in float (propagation.c:662, :681) */
 float fwi_src_term_f32(float src, float K, float dt, float invdx, float invdz);
+/* model operations of the FWI loop, acoustic2d_fwi.c:428-465, on [nx][nz] arrays:
+ * trial:  vp = 1/(slow + perturb), water layer, clip, Gardner rho (310 vp^0.25), water, clip
+ * update: slow += steplen*perturb, vp = 1/slow, water, clip, Gardner, water, clip, slow = 1/vp */
+void fwi_model_trial(const float *slow, const float *perturb, float *vp, float *rho, int nx, int nz, int waterdepth,
+                     float vp_water, float rho_water, float vpmin, float vpmax, float rhomin, float rhomax, int gardner);
+void fwi_model_update(float *slow, float *vp, float *rho, const float *perturb, float steplen, int nx, int nz,
+                      int waterdepth, float vp_water, float rho_water, float vpmin, float vpmax, float rhomin,
+                      float rhomax, int gardner);
 /* cosine taper coefficients 0.5(1+cos(pi*i/L)), i = 0..L (common.c:826-831) */
 void fwi_taper_coefs(int L, float *out);
 

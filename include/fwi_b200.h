@@ -179,6 +179,43 @@ typedef struct {
 } fwi_stats;
 FWI_API int fwi_ctx_stats(fwi_ctx *ctx, fwi_stats *out);
 
+/* one iteration of the FWI loop of acoustic2d_fwi.c:411-465 on the context's model, shots and
+ * observed data, everything between the two propagations on the device:
+ * gradient (problem 1) -> cos^2 smoothing along z (rz) then x (rx) -> fun1 = misfit ->
+ * histogram-scaled perturbation of the slowness -> trial model -> forward + residual
+ * (problem 2) -> fun2 -> step length -> model update.  The updated model stays in the
+ * context (fwi_ctx_get_model).  The slowness is carried between iterations as the
+ * reference carries it; the first call derives it from the model. */
+typedef struct {
+    int rx, rz;                 /* smoothing half-widths (x, z) */
+    int precondition;           /* pseudo-Hessian preconditioning */
+    int filter;                 /* residual filter: 2 (tapers only) */
+    float freq;                 /* taper reference frequency (0: wavelet peak) */
+    int waterdepth;             /* rows kept at the water values */
+    float vp_water, rho_water;
+    float vpmin, vpmax, rhomin, rhomax;
+    int gardner;                /* 1: rho from vp by Gardner after each update */
+    int path;                   /* FWI_PATH_PLAIN or FWI_PATH_BATCHED */
+} fwi_iter_params;
+typedef struct {
+    float fun1, fun2, steplen, scalar;
+    double ms;                  /* device time of the iteration (CUDA events) */
+    double cell_updates;
+    long long kernel_launches;
+} fwi_iter_result;
+FWI_API int fwi_ctx_fwi_iteration(fwi_ctx *ctx, const fwi_iter_params *p, fwi_iter_result *out);
+/* current model and gradient of the context (host arrays [nx][nz]) */
+FWI_API int fwi_ctx_get_model(fwi_ctx *ctx, float *vp, float *rho);
+
+/* the launch program of one shot's adjoint pass (host-only, no device needed): four ints per
+ * launch {kindA, stepA, kindB, stepB} with kinds 0 none, 3 replay step, 4 adjoint step.
+ * overlap 0 is the reference's order (a segment is replayed when the reverse loop reaches it,
+ * propagation.c:641-673); overlap 1 replays segment k-1 alongside the adjoint steps of segment k.
+ * Returns the number of launches; writes at most cap launches when items is not NULL. */
+FWI_API int fwi_adjoint_program(int nt, int overlap, int *items, int cap);
+/* checkpoint interval d = max(round(sqrt(2(nt-1))), 3) of checkpoint.c:47 */
+FWI_API int fwi_checkpoint_interval(int nt);
+
 #ifdef __cplusplus
 }
 #endif
