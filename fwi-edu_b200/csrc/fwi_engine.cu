@@ -33,6 +33,7 @@
 #include "fwi_kernels.cuh"
 #include "fwi_setup.h"
 #include "fwi_step.cuh"
+#include "fwi_optim.cuh"
 
 using namespace fwi;
 
@@ -110,7 +111,8 @@ struct fwi_ctx {
     bool host_model_valid = false;
     // shots
     std::vector<ShotHost> shots;
-    std::vector<float *> d_obs, d_pre;
+    std::vector<float *> d_obs, d_pre, d_pre_alt;  // d_pre_alt: the other gather set of a line search
+    std::vector<float> slow;                        // slowness carried by the FWI iteration
     std::vector<std::unique_ptr<Plan>> plans;
     std::vector<std::unique_ptr<ShotRun>> runs;  // one per shot (batched) or one reused (plain)
     ShotDesc *d_desc = nullptr;
@@ -199,6 +201,7 @@ extern "C" int fwi_ctx_destroy(fwi_ctx *c)
     }
     for (float *p : c->d_obs) cudaFree(p);
     for (float *p : c->d_pre) cudaFree(p);
+    for (float *p : c->d_pre_alt) cudaFree(p);
     cudaFree(c->d_vp); cudaFree(c->d_rho); cudaFree(c->d_grad); cudaFree(c->d_prec);
     cudaFree(c->d_gc); cudaFree(c->d_hc); cudaFree(c->d_red); cudaFree(c->d_scratch); cudaFree(c->d_desc);
     cudaEventDestroy(c->ev0); cudaEventDestroy(c->ev1);
@@ -306,8 +309,10 @@ extern "C" int fwi_ctx_set_shots(fwi_ctx *c, const fwi_shot *shots, int nshot)
     free_runs(c);
     for (float *p : c->d_obs) dfree(c, p, 0);
     for (float *p : c->d_pre) dfree(c, p, 0);
+    for (float *p : c->d_pre_alt) dfree(c, p, 0);
     c->d_obs.clear();
     c->d_pre.clear();
+    c->d_pre_alt.clear();
     c->shots.clear();
     for (int i = 0; i < nshot; i++) {
         ShotHost h;
@@ -327,6 +332,10 @@ extern "C" int fwi_ctx_set_shots(fwi_ctx *c, const fwi_shot *shots, int nshot)
         CK(cudaMemsetAsync(p, 0, nb, c->stream));
         c->d_obs.push_back(o);
         c->d_pre.push_back(p);
+        float *a = nullptr;
+        TRY(dmalloc(c, (void **)&a, nb));
+        CK(cudaMemsetAsync(a, 0, nb, c->stream));
+        c->d_pre_alt.push_back(a);
     }
     return FWI_OK;
 }
@@ -1278,4 +1287,149 @@ extern "C" void iso_acoustic2d_propagation_engine(Record2D *r, Acoustic2dCheckPo
                                                    iter, verbose, grad);
     if (rc != FWI_OK)
         fprintf(stderr, "<error>: iso_acoustic2d_propagation_engine failed (status %d): %s\n", rc, g_err.c_str());
+}
+
+// ------------------------------------------------------------------ FWI iteration
+extern "C" int fwi_ctx_get_model(fwi_ctx *c, float *vp, float *rho)
+{
+    if (!c || !vp || !rho || !c->host_model_valid) return fail(FWI_ERR_ARG, "no model");
+    memcpy(vp, c->vp.data(), c->vp.size() * 4);
+    memcpy(rho, c->rho.data(), c->rho.size() * 4);
+    return FWI_OK;
+}
+
+static std::vector<float> smooth_weights(int N)
+{
+    std::vector<float> w(2 * N + 1);
+    for (int i = 0; i < 2 * N + 1; i++) {  // common.c:955-961: double cosine, squared in float
+        w[i] = (float)cos(3.141592653589793 * (i - N) / (2.0 * N));
+        w[i] *= w[i];
+    }
+    return w;
+}
+
+static int sum_gathers(fwi_ctx *c, const std::vector<float *> &a, const std::vector<float *> *b, int op, double *s0,
+                       double *s1)
+{
+    *s0 = 0.0;
+    if (s1) *s1 = 0.0;
+    std::vector<SumDesc> sd;
+    for (size_t i = 0; i < c->shots.size(); i++) {
+        SumDesc d{};
+        d.a = a[i];
+        d.b = b ? (*b)[i] : nullptr;
+        d.n = (long long)c->shots[i].s.ntr * c->shots[i].s.ns;
+        d.op = op;
+        sd.push_back(d);
+    }
+    for (size_t i0 = 0; i0 < sd.size(); i0 += 64) {
+        std::vector<SumDesc> part(sd.begin() + i0, sd.begin() + std::min(sd.size(), i0 + 64));
+        std::vector<double> h;
+        TRY(reduce(c, part, h));
+        for (size_t i = 0; i < part.size(); i++) {  // shots in order, as the reference's outer loop
+            *s0 += h[2 * i];
+            if (s1) *s1 += h[2 * i + 1];
+        }
+    }
+    return FWI_OK;
+}
+
+// one pass of the loop body of acoustic2d_fwi.c:411-465
+extern "C" int fwi_ctx_fwi_iteration(fwi_ctx *c, const fwi_iter_params *p, fwi_iter_result *out)
+{
+    if (!c || !p || !out) return fail(FWI_ERR_ARG, "NULL argument");
+    if (!c->host_model_valid || c->shots.empty()) return fail(FWI_ERR_STATE, "set the model, shots and data first");
+    if (p->rx < 1 || p->rz < 1) return fail(FWI_ERR_ARG, "smoothing half-widths must be >= 1");
+    CK(cudaSetDevice(c->device));
+    const int nx = c->nx, nz = c->nz;
+    const size_t m = (size_t)nx * nz;
+    cudaEvent_t e0, e1;
+    CK(cudaEventCreate(&e0));
+    CK(cudaEventCreate(&e1));
+    CK(cudaEventRecord(e0, c->stream));
+    long long l0 = c->launches;
+    if (c->slow.size() != m) {  // v2slow of the starting model (acoustic2d_fwi.c:365)
+        c->slow.resize(m);
+        for (size_t i = 0; i < m; i++) c->slow[i] = c->vp[i] != 0.0f ? 1.0f / c->vp[i] : 0.0f;
+    }
+    // gradient
+    TRY(fwi_ctx_run(c, 1, p->freq, p->filter, p->precondition, p->path));
+    double cells = c->stats.cell_updates;
+    // smoothing along z then x (acoustic2d_fwi.c:418-419), fun1, perturbation, all on the device
+    std::vector<float> wz = smooth_weights(p->rz), wx = smooth_weights(p->rx);
+    float *d_work;
+    const size_t nb = ((m * 4 + 255) / 256) * 256;
+    TRY(scratch(c, 3 * nb + 4096 + sizeof(PertState) + 1024, (void **)&d_work));
+    float *d_tmp = d_work, *d_slow = (float *)((char *)d_work + nb), *d_pert = (float *)((char *)d_work + 2 * nb);
+    float *d_w = (float *)((char *)d_work + 3 * nb);
+    PertState *d_st = (PertState *)((char *)d_work + 3 * nb + 4096);
+    if ((size_t)(2 * p->rz + 1 + 2 * p->rx + 1) * 4 > 4096) return fail(FWI_ERR_ARG, "smoothing window too wide");
+    CK(cudaMemcpyAsync(d_w, wz.data(), wz.size() * 4, cudaMemcpyHostToDevice, c->stream));
+    CK(cudaMemcpyAsync(d_w + wz.size(), wx.data(), wx.size() * 4, cudaMemcpyHostToDevice, c->stream));
+    k_smooth2d<<<592, 256, 0, c->stream>>>(c->d_grad, d_tmp, nx, nz, p->rz, 1, d_w);
+    k_smooth2d<<<592, 256, 0, c->stream>>>(d_tmp, c->d_grad, nx, nz, p->rx, 0, d_w + wz.size());
+    c->launches += 2;
+    double f1;
+    TRY(sum_gathers(c, c->d_pre, nullptr, 1, &f1, nullptr));
+    const float fun1 = (float)(0.5 * f1);
+    CK(cudaMemcpyAsync(d_slow, c->slow.data(), m * 4, cudaMemcpyHostToDevice, c->stream));
+    SumDesc sd{};
+    sd.a = d_slow;
+    sd.n = (long long)m;
+    sd.op = 0;
+    std::vector<double> hs;
+    double *d_ssum;
+    TRY(reduce(c, {sd}, hs, &d_ssum));
+    k_pert_init<<<1, 256, 0, c->stream>>>(d_st);
+    k_pert_minmax<<<296, 256, 0, c->stream>>>(c->d_grad, (long long)m, d_st);
+    k_pert_hist<<<296, 256, 0, c->stream>>>(c->d_grad, (long long)m, d_st);
+    k_pert_scalar<<<1, 32, 0, c->stream>>>(d_st, d_ssum, (long long)m, 0.01f);
+    k_pert_apply<<<296, 256, 0, c->stream>>>(c->d_grad, d_pert, (long long)m, d_st);
+    c->launches += 5;
+    CK(cudaGetLastError());
+    std::vector<float> pert(m);
+    float scalar = 0.0f;
+    CK(cudaMemcpyAsync(pert.data(), d_pert, m * 4, cudaMemcpyDeviceToHost, c->stream));
+    CK(cudaMemcpyAsync(&scalar, &d_st->scalar, 4, cudaMemcpyDeviceToHost, c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+    // the output gradient has its water rows zeroed (acoustic2d_fwi.c:425)
+    for (int ix = 0; ix < nx && p->waterdepth > 0; ix++)
+        CK(cudaMemsetAsync(c->d_grad + (size_t)ix * nz, 0, (size_t)std::min(p->waterdepth, nz) * 4, c->stream));
+    // trial model on the host with the C library's powf (Gardner), then the line-search forward
+    std::vector<float> vp0 = c->vp, rho0 = c->rho, vpt(m), rhot(m);
+    rhot = rho0;
+    fwi_model_trial(c->slow.data(), pert.data(), vpt.data(), rhot.data(), nx, nz, p->waterdepth, p->vp_water,
+                    p->rho_water, p->vpmin, p->vpmax, p->rhomin, p->rhomax, p->gardner);
+    TRY(fwi_ctx_set_model(c, vpt.data(), rhot.data(), nz, nx, c->dx, c->dz, c->dt, c->nt, c->pml, c->fs));
+    std::swap(c->d_pre, c->d_pre_alt);  // keep the gradient's residuals: problem 2 writes the other set
+    int rc = fwi_ctx_run(c, 2, p->freq, p->filter, p->precondition, p->path);
+    if (rc != FWI_OK) {
+        std::swap(c->d_pre, c->d_pre_alt);
+        return rc;
+    }
+    cells += c->stats.cell_updates;
+    double f2, num, den;
+    TRY(sum_gathers(c, c->d_pre, nullptr, 1, &f2, nullptr));
+    TRY(sum_gathers(c, c->d_pre_alt, &c->d_pre, 3, &num, &den));
+    const float fun2 = (float)(0.5 * f2);
+    const float steplen = den == 0.0 ? 0.0f : (float)(num / den);
+    // model update (acoustic2d_fwi.c:452-465)
+    std::vector<float> vpn = vp0, rhon = rho0;
+    fwi_model_update(c->slow.data(), vpn.data(), rhon.data(), pert.data(), steplen, nx, nz, p->waterdepth,
+                     p->vp_water, p->rho_water, p->vpmin, p->vpmax, p->rhomin, p->rhomax, p->gardner);
+    TRY(fwi_ctx_set_model(c, vpn.data(), rhon.data(), nz, nx, c->dx, c->dz, c->dt, c->nt, c->pml, c->fs));
+    CK(cudaEventRecord(e1, c->stream));
+    CK(cudaEventSynchronize(e1));
+    float ms = 0.f;
+    CK(cudaEventElapsedTime(&ms, e0, e1));
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    out->fun1 = fun1;
+    out->fun2 = fun2;
+    out->steplen = steplen;
+    out->scalar = scalar;
+    out->ms = ms;
+    out->cell_updates = cells;
+    out->kernel_launches = c->launches - l0;
+    return FWI_OK;
 }

@@ -59,6 +59,19 @@ class FwiStats(C.Structure):
                 ("graph_launches", C.c_longlong), ("device_bytes", C.c_size_t)]
 
 
+class IterParams(C.Structure):
+    """fwi_iter_params: one iteration of the FWI loop (acoustic2d_fwi.c:411-465)."""
+    _fields_ = [("rx", C.c_int), ("rz", C.c_int), ("precondition", C.c_int), ("filter", C.c_int),
+                ("freq", C.c_float), ("waterdepth", C.c_int), ("vp_water", C.c_float), ("rho_water", C.c_float),
+                ("vpmin", C.c_float), ("vpmax", C.c_float), ("rhomin", C.c_float), ("rhomax", C.c_float),
+                ("gardner", C.c_int), ("path", C.c_int)]
+
+
+class IterResult(C.Structure):
+    _fields_ = [("fun1", C.c_float), ("fun2", C.c_float), ("steplen", C.c_float), ("scalar", C.c_float),
+                ("ms", C.c_double), ("cell_updates", C.c_double), ("kernel_launches", C.c_longlong)]
+
+
 _lib = None
 _lock = threading.Lock()
 
@@ -233,6 +246,17 @@ class Context:
         v = C.c_double()
         _check(self.L.fwi_ctx_objective(self.h, C.byref(v)))
         return v.value
+
+    def fwi_iteration(self, params: IterParams):
+        r = IterResult()
+        _check(self.L.fwi_ctx_fwi_iteration(self.h, C.byref(params), C.byref(r)))
+        return {k: getattr(r, k) for k, _ in IterResult._fields_}
+
+    def model(self):
+        vp = np.empty((self.nx, self.nz), np.float32)
+        rho = np.empty_like(vp)
+        _check(self.L.fwi_ctx_get_model(self.h, _ptr(vp), _ptr(rho)))
+        return vp, rho
 
     def stats(self):
         s = FwiStats()

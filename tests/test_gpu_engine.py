@@ -182,3 +182,35 @@ def test_context_api_gradient_and_objective(port32):
     st = ctx.stats()
     assert st["kernel_launches"] > c.nt and st["cell_updates"] > 0
     ctx.close()
+
+
+def test_fwi_iteration_matches_oracle(port32):
+    """fwi_ctx_fwi_iteration against the oracle composed step by step (acoustic2d_fwi.c:411-465)."""
+    c = Case("fs1_small")
+    P = dict(rx=2, rz=1, precondition=1, filter=2, freq=10.0, waterdepth=6, vp_water=1500.0, rho_water=1000.0,
+             vpmin=1500.0, vpmax=4700.0, rhomin=1000.0, rhomax=2700.0, gardner=1)
+    ctx = E.Context(0)
+    ctx.set_model(c.vp0, c.rho0, c.dx, c.dx, c.dt, c.nt, c.pml, c.fs)
+    ctx.set_shots(c.shots)
+    ctx.set_observed(c.obs)
+    r = ctx.fwi_iteration(E.IterParams(path=E.PATH_BATCHED, **P))
+    vp_g, rho_g = ctx.model()
+    ctx.close()
+    # oracle
+    slow = np.where(c.vp0 != 0, 1.0 / c.vp0, 0).astype(np.float32)
+    pre0, grad = port32.propagation(c.vp0, c.rho0, c.shots, c.dx, c.dx, c.dt, c.nt, c.pml, c.fs, 10.0, 2.0, 1, 1,
+                                    obs=c.obs)
+    g = port32.smooth2d(port32.smooth2d(grad, P["rz"], 1), P["rx"], 0)
+    fun1 = port32.objective(pre0)
+    scalar, pert = port32.model_perturbation(0.01, slow, g)
+    vpt, rhot = port32.fwi_trial(slow, pert, 6, 1500.0, 1000.0, 1500.0, 4700.0, 1000.0, 2700.0)
+    pre1, _ = port32.propagation(vpt, rhot, c.shots, c.dx, c.dx, c.dt, c.nt, c.pml, c.fs, 10.0, 2.0, 1, 2, obs=c.obs)
+    fun2 = port32.objective(pre1)
+    steplen = port32.step_length(pre0, pre1)
+    slow2, vp2, rho2 = port32.fwi_update(slow, c.vp0, c.rho0, pert, steplen, 6, 1500.0, 1000.0, 1500.0, 4700.0,
+                                         1000.0, 2700.0)
+    assert np.float32(r["fun1"]) == np.float32(fun1)
+    assert np.float32(r["fun2"]) == np.float32(fun2)
+    assert np.float32(r["scalar"]) == np.float32(scalar)
+    assert abs(r["steplen"] - steplen) <= 1e-6 * abs(steplen)
+    assert rel(vp_g, vp2) <= 1e-6 and rel(rho_g, rho2) <= 1e-6
