@@ -207,6 +207,20 @@ FWI_API int fwi_ctx_fwi_iteration(fwi_ctx *ctx, const fwi_iter_params *p, fwi_it
 /* current model and gradient of the context (host arrays [nx][nz]) */
 FWI_API int fwi_ctx_get_model(fwi_ctx *ctx, float *vp, float *rho);
 
+/* Two-pass cos^2 smoothing of a device-resident [nx][nz] field -- a z pass with half-width rz, then
+ * an x pass with rx, each computed as smooth2D computes it -- that allocates no memory.  It has no
+ * counterpart in the reference.  It is meant for callers that cannot call cudaMalloc: a serving
+ * loop that has reserved its whole device budget up front, host code that runs between the
+ * segments of a captured CUDA graph, or a latency-critical loop where an allocation would
+ * synchronise the device.  d_in and d_out are the caller's device arrays (they may not overlap);
+ * the intermediate field lives in a file-scope device array of 4194304 floats (16 MiB) that every
+ * GPU loading this library holds until the process exits.  nx*nz above 4194304 or half-widths
+ * outside [1, 32] are rejected with FWI_ERR_ARG and a message.  The first call on a device looks up
+ * the array's address on that device (with that device current): make that first call before any
+ * stream capture.  All calls share the array, so calls that overlap on the GPU race on it.
+ * stream is a cudaStream_t (NULL: the legacy default stream); the call only enqueues work. */
+FWI_API int fwi_smooth2d_noalloc(const float *d_in, float *d_out, int nx, int nz, int rz, int rx, void *stream);
+
 /* the launch program of one shot's adjoint pass (host-only, no device needed): four ints per
  * launch {kindA, stepA, kindB, stepB} with kinds 0 none, 3 replay step, 4 adjoint step.
  * overlap 0 is the reference's order (a segment is replayed when the reverse loop reaches it,
