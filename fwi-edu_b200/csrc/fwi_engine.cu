@@ -14,6 +14,8 @@
 // group go into every launch and the whole launch sequence is captured once as
 // a CUDA graph and replayed; on the plain path shots run one after another, one
 // launch per step, as the reference's shot loop does (propagation.c:857, :895).
+#include <cuda.h>
+#include <cudaTypedefs.h>  // PFN_cuTensorMapEncodeTiled
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -25,6 +27,7 @@
 #include <deque>
 #include <map>
 #include <memory>
+#include <mutex>
 #include <string>
 #include <vector>
 
@@ -33,6 +36,7 @@
 #include "fwi_kernels.cuh"
 #include "fwi_setup.h"
 #include "fwi_step.cuh"
+#include "fwi_tile.cuh"
 #include "fwi_optim.cuh"
 
 using namespace fwi;
@@ -128,6 +132,7 @@ struct fwi_ctx {
     std::map<std::string, cudaGraphExec_t> graphs;
     fwi_stats stats{};
     int math = 0;  // 0: bit-exact arithmetic, 1: contracted multiply-adds
+    int *d_err = nullptr;  // set by a step kernel whose tile copy did not complete
     long long launches = 0;
     double last_obj = 0.0;
 };
@@ -184,6 +189,8 @@ extern "C" int fwi_ctx_create(fwi_ctx **out, int device, size_t budget)
     CK(cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking));
     CK(cudaEventCreate(&c->ev0));
     CK(cudaEventCreate(&c->ev1));
+    CK(cudaMalloc((void **)&c->d_err, sizeof(int)));
+    CK(cudaMemset(c->d_err, 0, sizeof(int)));
     *out = c;
     return FWI_OK;
 }
@@ -204,6 +211,7 @@ extern "C" int fwi_ctx_destroy(fwi_ctx *c)
     for (float *p : c->d_pre_alt) cudaFree(p);
     cudaFree(c->d_vp); cudaFree(c->d_rho); cudaFree(c->d_grad); cudaFree(c->d_prec);
     cudaFree(c->d_gc); cudaFree(c->d_hc); cudaFree(c->d_red); cudaFree(c->d_scratch); cudaFree(c->d_desc);
+    cudaFree(c->d_err);
     cudaEventDestroy(c->ev0); cudaEventDestroy(c->ev1);
     cudaStreamDestroy(c->stream);
     delete c;
@@ -400,6 +408,49 @@ static int ralloc(fwi_ctx *c, ShotRun *r, void **p, size_t bytes)
     return FWI_OK;
 }
 
+// ---------------------------------------------------------------- TMA descriptors
+// cuTensorMapEncodeTiled through the runtime's driver entry point (no libcuda link)
+static PFN_cuTensorMapEncodeTiled_v12000 tensor_map_encoder()
+{
+    static std::once_flag once;
+    static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
+    std::call_once(once, [] {
+        void *p = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            fn = (PFN_cuTensorMapEncodeTiled_v12000)p;
+    });
+    return fn;
+}
+
+// 3-D float map {d0 (z, contiguous), d1 (x), d2 (frames or planes)}, box {b0, b1, b2};
+// out-of-range elements of a box read as zero
+static int encode_map(CUtensorMap *m, const float *base, int d0, int d1, int d2, int b0, int b1, int b2)
+{
+    PFN_cuTensorMapEncodeTiled_v12000 enc = tensor_map_encoder();
+    if (!enc) return fail(FWI_ERR_CUDA, "cuTensorMapEncodeTiled is not available from the driver");
+    const cuuint64_t dims[3] = {(cuuint64_t)d0, (cuuint64_t)d1, (cuuint64_t)d2};
+    const cuuint64_t strides[2] = {(cuuint64_t)d0 * 4, (cuuint64_t)d0 * d1 * 4};
+    const cuuint32_t box[3] = {(cuuint32_t)b0, (cuuint32_t)b1, (cuuint32_t)b2}, es[3] = {1, 1, 1};
+    CUresult r = enc(m, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 3, (void *)base, dims, strides, box, es,
+                     CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+                     CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    if (r != CUDA_SUCCESS) return fail(FWI_ERR_CUDA, "cuTensorMapEncodeTiled failed (%d)", (int)r);
+    return FWI_OK;
+}
+
+template <int TX>
+static int encode_tile_maps(ShotDesc &d, const float *coef)
+{
+    using Geo = TileGeom<TX>;
+    constexpr int w = tile_w<TX>();
+    TRY(encode_map(&d.tm_p1[w], d.frames, d.ld, d.Nx, d.nfr, Geo::ZP, Geo::XP, 1));
+    TRY(encode_map(&d.tm_p0[w], d.frames, d.ld, d.Nx, d.nfr, Geo::ZC, TX, 1));
+    TRY(encode_map(&d.tm_cf[w], coef, d.ld, d.Nx, 6, Geo::ZC, TX, 6));
+    return FWI_OK;
+}
+
 // fill the geometry/coefficients part of a descriptor; allocate what the run needs
 static int prepare_run(fwi_ctx *c, ShotRun *r, int shot, bool gradient)
 {
@@ -426,6 +477,7 @@ static int prepare_run(fwi_ctx *c, ShotRun *r, int shot, bool gradient)
     d.isx = s.isx + c->pml; d.isz = s.isz + c->pml;
     d.invdx = hc.invdx; d.invdz = hc.invdz; d.invdxdx = hc.invdxdx; d.invdzdz = hc.invdzdz;
     d.invdtdt = hc.invdtdt; d.dt = c->dt;
+    d.negzero = -0.0f;
     const size_t fr = p->frame();
     d.frame = (long long)fr;
     d.c1 = p->d_coef; d.c2 = p->d_coef + fr; d.ck = p->d_coef + 2 * fr;
@@ -440,15 +492,11 @@ static int prepare_run(fwi_ctx *c, ShotRun *r, int shot, bool gradient)
         TRY(ralloc(c, r, &q, (size_t)ntr * 4)); d.recK = (float *)q;
         TRY(ralloc(c, r, &q, (size_t)ntr * 4)); d.rec_off = (int *)q;
         TRY(ralloc(c, r, &q, (size_t)s.ns * ntr * 4)); d.traces_t = (float *)q;
-        TRY(ralloc(c, r, &q, 3 * fr * 4)); d.fscr = (float *)q;
-        d.ckslots = d.rscr = d.seg = d.ascr = nullptr;
+        d.nfr = gradient ? nframes_gradient(d.K, d.S5) : 3;
+        TRY(ralloc(c, r, &q, (size_t)d.nfr * fr * 4)); d.frames = (float *)q;
         d.H = d.Gacc = nullptr;
         d.adj_t = nullptr;
         if (gradient) {
-            TRY(ralloc(c, r, &q, (size_t)(2 * (d.K + 1)) * fr * 4)); d.ckslots = (float *)q;
-            TRY(ralloc(c, r, &q, 3 * fr * 4)); d.rscr = (float *)q;
-            TRY(ralloc(c, r, &q, (size_t)(2 * d.S5) * fr * 4)); d.seg = (float *)q;
-            TRY(ralloc(c, r, &q, 3 * fr * 4)); d.ascr = (float *)q;
             TRY(ralloc(c, r, &q, fr * 8)); d.H = (double *)q;
             TRY(ralloc(c, r, &q, fr * 8)); d.Gacc = (double *)q;
             TRY(ralloc(c, r, &q, (size_t)nt * ntr * 4)); d.adj_t = (float *)q;
@@ -493,6 +541,14 @@ static int prepare_run(fwi_ctx *c, ShotRun *r, int shot, bool gradient)
         colptr[X + 1]++;
     }
     for (int x = 0; x < d.Nx; x++) colptr[x + 1] += colptr[x];
+    d.rz0 = 1 << 30;
+    d.rz1 = -1;
+    for (int i = 0; i < ntr; i++) {
+        d.rz0 = std::min(d.rz0, sh.igz[i] + c->pml);
+        d.rz1 = std::max(d.rz1, sh.igz[i] + c->pml);
+    }
+    TRY(encode_tile_maps<8>(d, p->d_coef));
+    TRY(encode_tile_maps<16>(d, p->d_coef));
     CK(cudaMemcpyAsync((void *)d.srcd, sd.data(), nt * 8, cudaMemcpyHostToDevice, c->stream));
     CK(cudaMemcpyAsync((void *)d.srcf, sf.data(), nt * 4, cudaMemcpyHostToDevice, c->stream));
     CK(cudaMemcpyAsync((void *)d.colptr, colptr.data(), (d.Nx + 1) * 4, cudaMemcpyHostToDevice, c->stream));
@@ -648,22 +704,97 @@ static LaunchCfg pick_launch(int Nx, int nshot, bool batched, int math)
     return L;
 }
 
+typedef void (*TileFn)(const ShotDesc *, const int4 *, int, int, int, int, int *);
+
+template <int TX, int NST, int MATH>
+static TileFn tile_fn()
+{
+    static bool ready = false;
+    TileFn f = k_tile<TX, NST, MATH>;
+    if (!ready) {
+        cudaFuncSetAttribute((const void *)f, cudaFuncAttributeMaxDynamicSharedMemorySize, TileGeom<TX>::smem(NST));
+        cudaFuncSetAttribute((const void *)f, cudaFuncAttributePreferredSharedMemoryCarveout,
+                             cudaSharedmemCarveoutMaxShared);
+        ready = true;
+    }
+    return f;
+}
+
+template <int TX, int MATH>
+static TileFn tile_fn_nst(int nst)
+{
+    return nst == 2 ? tile_fn<TX, 2, MATH>() : nst == 4 ? tile_fn<TX, 4, MATH>() : tile_fn<TX, 3, MATH>();
+}
+
+// shots per block: the most (up to TILE_CH_MAX) whose grid still fills the last wave of
+// resident blocks about as well as the best choice does
+static int pick_chunk(int tiles, int nshot, int resident)
+{
+    const int slots = 148 * resident;
+    auto fill = [&](int ch) {
+        const long long blocks = (long long)tiles * ((nshot + ch - 1) / ch);
+        const long long waves = (blocks + slots - 1) / slots;
+        return (double)blocks / (double)(waves * slots);
+    };
+    double best = 0.0;
+    for (int ch = 1; ch <= std::min(nshot, TILE_CH_MAX); ch++) best = std::max(best, fill(ch));
+    int pick = 1;
+    for (int ch = 1; ch <= std::min(nshot, TILE_CH_MAX); ch++)
+        if (fill(ch) >= 0.9 * best) pick = ch;
+    return pick;
+}
+
 static int launch_steps(fwi_ctx *c, const Program *prog, int shot_base, int nshot, int prog_stride, const Plan *p,
                         bool batched)
 {
     (void)prog_stride;
-    LaunchCfg cfg = pick_launch(p->Nx, nshot, batched, c->math);
     const int zt = (p->G + TG - 1) / TG;
-    const int groups = (nshot + cfg.S - 1) / cfg.S;
-    dim3 grid((p->Nx + cfg.tx - 1) / cfg.tx + 1, 2 * groups, zt);
     const int n = (int)prog->items.size();
+    const char *ke = getenv("FWI_KERNEL");  // "step": the cp.async kernel, kept for comparison
+    if (ke && strcmp(ke, "step") == 0) {
+        LaunchCfg cfg = pick_launch(p->Nx, nshot, batched, c->math);
+        const int groups = (nshot + cfg.S - 1) / cfg.S;
+        dim3 grid((p->Nx + cfg.tx - 1) / cfg.tx + 1, 2 * groups, zt);
+        for (int L = 0; L < n; L++) {
+            const int4 &pw = prog->items[L];
+            if (pw.x == K_NONE && pw.z == K_NONE) continue;
+            cfg.fn<<<grid, dim3(TG, TYX), 0, c->stream>>>(c->d_desc, prog->d, L, shot_base, nshot);
+            c->launches++;
+        }
+        CK(cudaGetLastError());
+        return FWI_OK;
+    }
+    int tx = batched ? 16 : 8;
+    if (const char *e = getenv("FWI_TX")) tx = atoi(e) == 8 ? 8 : 16;
+    int nst = tx == 16 ? 3 : 4;
+    if (const char *e = getenv("FWI_NST")) nst = std::min(4, std::max(2, atoi(e)));
+    const int ntx = (p->Nx + tx - 1) / tx;
+    int chunk = pick_chunk(ntx * zt, nshot, tx == 16 ? 2 : 4);
+    if (const char *e = getenv("FWI_CHUNK")) chunk = std::min(TILE_CH_MAX, std::max(1, atoi(e)));
+    TileFn fn = tx == 16 ? (c->math ? tile_fn_nst<16, 1>(nst) : tile_fn_nst<16, 0>(nst))
+                         : (c->math ? tile_fn_nst<8, 1>(nst) : tile_fn_nst<8, 0>(nst));
+    const int smem = tx == 16 ? TileGeom<16>::smem(nst) : TileGeom<8>::smem(nst);
+    const int nchunks = (nshot + chunk - 1) / chunk;
+    dim3 grid(ntx + 1, 2 * nchunks, zt);
     for (int L = 0; L < n; L++) {
         const int4 &pw = prog->items[L];
         if (pw.x == K_NONE && pw.z == K_NONE) continue;
-        cfg.fn<<<grid, dim3(TG, TYX), 0, c->stream>>>(c->d_desc, prog->d, L, shot_base, nshot);
+        fn<<<grid, dim3(TG, tx), smem, c->stream>>>(c->d_desc, prog->d, L, shot_base, nshot, chunk, c->d_err);
         c->launches++;
     }
     CK(cudaGetLastError());
+    return FWI_OK;
+}
+
+// a step kernel that gave up waiting for a tile copy leaves its mark in the error word
+static int check_kernel_error(fwi_ctx *c)
+{
+    int e = 0;
+    CK(cudaMemcpy(&e, c->d_err, sizeof(int), cudaMemcpyDeviceToHost));
+    if (e) {
+        CK(cudaMemset(c->d_err, 0, sizeof(int)));
+        return fail(FWI_ERR_CUDA, "step kernel: a tile copy did not complete within 2 s; results are invalid");
+    }
     return FWI_OK;
 }
 
@@ -862,9 +993,9 @@ static int stack_and_precondition(fwi_ctx *c, const std::vector<ShotRun *> &rs, 
 static int zero_initial(fwi_ctx *c, ShotRun *r, bool gradient)
 {
     const size_t fb = (size_t)r->d.frame * 4;
-    CK(cudaMemsetAsync(r->d.fscr, 0, 3 * fb, c->stream));
+    CK(cudaMemsetAsync(frame_ptr(r->d, F_FWD), 0, 3 * fb, c->stream));
     if (gradient) {
-        CK(cudaMemsetAsync(r->d.ckslots, 0, 2 * fb, c->stream));  // u(-1), u(0)
+        CK(cudaMemsetAsync(frame_ptr(r->d, F_CK), 0, 2 * fb, c->stream));  // u(-1), u(0)
         CK(cudaMemsetAsync(r->d.H, 0, (size_t)r->d.frame * 8, c->stream));
         CK(cudaMemsetAsync(r->d.Gacc, 0, (size_t)r->d.frame * 8, c->stream));
     }
@@ -1067,6 +1198,7 @@ extern "C" int fwi_ctx_run(fwi_ctx *c, int problem, float freq, int filter, int 
     }
     CK(cudaEventRecord(c->ev1, c->stream));
     CK(cudaEventSynchronize(c->ev1));
+    TRY(check_kernel_error(c));
     float ms = 0.f;
     CK(cudaEventElapsedTime(&ms, c->ev0, c->ev1));
     for (int i = 0; i < ns; i++) {

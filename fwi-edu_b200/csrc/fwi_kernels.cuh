@@ -5,6 +5,7 @@
 // Fields are [Nx][ld] floats, z fastest, ld = Nz rounded up to 4 (16-byte rows).
 #pragma once
 #include <cstdint>
+#include <cuda.h>  // CUtensorMap (the encoded TMA descriptor type; no driver call is made here)
 #include <cuda_runtime.h>
 
 namespace fwi {
@@ -27,6 +28,7 @@ struct ShotDesc {
     int nt, d, K, ns, sr, ntr, S5, hessian;
     int isx, isz;  // padded source cell
     float invdx, invdz, invdxdx, invdzdz, invdtdt, dt;
+    float negzero;  // -0.0f, read at run time (the exact packed products are fma(a, b, -0))
     // coefficients [Nx][ld]
     const float *c1, *c2, *ck, *irx, *irz, *ir;
     // source terms per step: forward (double, propagation.c:558) and replay (float, :662)
@@ -39,14 +41,19 @@ struct ShotDesc {
     const int *rec_off;    // per receiver (trace order): padded cell offset X*ld + Z
     float *traces_t;       // [ns][ntr] samples of the forward pass
     const float *adj_t;    // [nt][ntr] adjoint source
-    // wavefield storage, each a sequence of frames of Nx*ld floats
-    float *ckslots;        // 2*(K+1) checkpoint frames: slot 0 = u(-1), 2k+1 = u(kd), 2k = u(kd-1)
-    float *fscr;           // 3 forward scratch frames
-    float *rscr;           // 3 replay scratch frames
-    float *seg;            // 2*S5 replayed frames kept for imaging (t % 5 == 0), double-buffered by segment
-    float *ascr;           // 3 adjoint frames
+    // wavefield storage: one block of nfr frames of Nx*ld floats per shot, laid out as
+    // F_FWD (3 forward frames), F_ADJ (3 adjoint), F_REP (3 replay), F_CK (2(K+1) checkpoint
+    // slots: slot 0 = u(-1), 2k+1 = u(kd), 2k = u(kd-1)), then 2*S5 replayed frames kept for
+    // imaging (t % 5 == 0), double-buffered by segment.  A forward-only run has nfr = 3.
+    float *frames;
+    int nfr;
     double *H, *Gacc;      // [Nx][ld] FP64 accumulators (pseudo-Hessian, gradient)
     long long frame;       // Nx*ld
+    int rz0, rz1;          // padded depth range of this shot's receivers
+    // TMA descriptors, per tile width w (0: 8 columns, 1: 16 columns): the p1 tile with its
+    // halo and the p0 tile over the frame block {ld, Nx, nfr}, and the six coefficient
+    // planes {ld, Nx, 6} of the shot's model window
+    CUtensorMap tm_p1[2], tm_p0[2], tm_cf[2];
 };
 
 // ------------------------------------------------------------ buffer selection
@@ -60,41 +67,47 @@ __host__ __device__ inline int stored_slot(const ShotDesc &S, int t)
     if ((t + 1) % S.d == 0 && t + 1 < S.nt) return 2 * ((t + 1) / S.d);
     return -1;
 }
-__host__ __device__ inline float *frame_at(float *base, long long frame, int i) { return base + (long long)i * frame; }
+constexpr int F_FWD = 0, F_ADJ = 3, F_REP = 6, F_CK = 9;
+__host__ __device__ inline int nframes_gradient(int K, int S5) { return F_CK + 2 * (K + 1) + 2 * S5; }
+__host__ __device__ inline float *frame_ptr(const ShotDesc &S, int i) { return S.frames + (long long)i * S.frame; }
 
-// forward field u(t) in a pass that keeps checkpoints (mode 1) or not (mode 0)
-__host__ __device__ inline float *fwd_buf(const ShotDesc &S, int t, bool keep)
+// frame of the forward field u(t) in a pass that keeps checkpoints (mode 1) or not (mode 0)
+__host__ __device__ inline int fwd_idx(const ShotDesc &S, int t, bool keep)
 {
     if (keep) {
         int s = stored_slot(S, t);
-        if (s >= 0) return frame_at(S.ckslots, S.frame, s);
+        if (s >= 0) return F_CK + s;
     }
-    return frame_at(S.fscr, S.frame, (t + 3) % 3);
+    return F_FWD + (t + 3) % 3;
 }
 // replayed frame of segment k (checkpoint c = k*d), t > c, t % 5 == 0
-__host__ __device__ inline float *seg_buf(const ShotDesc &S, int t)
+__host__ __device__ inline int seg_idx(const ShotDesc &S, int t)
 {
     int k = t / S.d, c = k * S.d;
     int j = t / MST - (c + MST) / MST;
-    return frame_at(S.seg, S.frame, (k & 1) * S.S5 + j);
+    return F_CK + 2 * (S.K + 1) + (k & 1) * S.S5 + j;
 }
 // u(t) during the replay of the segment containing t
-__host__ __device__ inline float *rep_buf(const ShotDesc &S, int t)
+__host__ __device__ inline int rep_idx(const ShotDesc &S, int t)
 {
     int s = stored_slot(S, t);
-    if (s >= 0) return frame_at(S.ckslots, S.frame, s);
-    if (t % MST == 0) return seg_buf(S, t);
-    return frame_at(S.rscr, S.frame, t % 3);
+    if (s >= 0) return F_CK + s;
+    if (t % MST == 0) return seg_idx(S, t);
+    return F_REP + t % 3;
 }
 // adjoint field A(t): p1 of adjoint step t (with the injection of step t applied)
-__host__ __device__ inline float *adj_buf(const ShotDesc &S, int t) { return frame_at(S.ascr, S.frame, (t + 3) % 3); }
+__host__ __device__ inline int adj_idx(const ShotDesc &, int t) { return F_ADJ + (t + 3) % 3; }
 // forward field used by the imaging condition at adjoint step it (it % 5 == 0)
-__host__ __device__ inline float *img_buf(const ShotDesc &S, int it)
+__host__ __device__ inline int img_idx(const ShotDesc &S, int it)
 {
     int s = stored_slot(S, it);
-    if (s >= 0) return frame_at(S.ckslots, S.frame, s);
-    return seg_buf(S, it);
+    if (s >= 0) return F_CK + s;
+    return seg_idx(S, it);
 }
+__host__ __device__ inline float *fwd_buf(const ShotDesc &S, int t, bool keep) { return frame_ptr(S, fwd_idx(S, t, keep)); }
+__host__ __device__ inline float *rep_buf(const ShotDesc &S, int t) { return frame_ptr(S, rep_idx(S, t)); }
+__host__ __device__ inline float *adj_buf(const ShotDesc &S, int t) { return frame_ptr(S, adj_idx(S, t)); }
+__host__ __device__ inline float *img_buf(const ShotDesc &S, int it) { return frame_ptr(S, img_idx(S, it)); }
 
 // ------------------------------------------------------------------ helpers
 __device__ __forceinline__ float4 ldg4(const float *p) { return __ldg(reinterpret_cast<const float4 *>(p)); }

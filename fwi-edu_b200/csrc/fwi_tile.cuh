@@ -1,0 +1,436 @@
+// fwi_tile.cuh -- the TMA-fed time-step kernel.
+//
+// A block owns one tile of the padded grid (TG = 16 float4 z-groups = 64 rows by TX
+// columns, one thread per group and column) and walks a chunk of shots that share
+// the model window.  The shots' fields never pass through registers on their way in:
+// one thread issues, per shot, two tensor copies (cp.async.bulk.tensor) -- the p1 tile
+// with its halo (one group above and below, three columns left and right) and the p0
+// tile -- into a ring of NST shared-memory stages, each completed on its own mbarrier,
+// so the loads of the next NST-1 shots run while the block computes the current one.
+// The six coefficient tiles arrive once per block, by one more tensor copy, and stay in
+// registers for all shots.  Out-of-range parts of a tile (grid edges) are zero-filled by
+// the copy engine.
+//
+// Arithmetic uses the packed f32x2 add/sub/mul of sm_100 on pairs of neighbouring cells,
+// with every operation rounded separately in the reference's association order: the
+// results are bit-identical to the scalar __fadd_rn/__fmul_rn evaluation of
+// acoustic_iso2d_fd_it_6order (propagation.c:13-74) and to the reference's strict IEEE
+// build (MATH 0).  MATH 1 contracts multiply-adds into packed FMAs (within the FP32
+// tolerance of the seismograms, not bitwise).
+//
+// The epilogue fuses what the reference does around the stencil: point source (forward:
+// double, before the free surface, propagation.c:558; replay: float, after it, :662),
+// mirror free surface (:76-101), pseudo-Hessian (:579-594), imaging (:700-714) and the
+// adjoint injection (:676-682).  Its branches are uniform over a tile wherever they can
+// be: only tiles that reach the free-surface rows, the source or the receiver rows take
+// the corresponding code.
+//
+// Every wait is bounded: a tile copy that has not landed after two seconds sets the
+// error word, the block waits (again bounded) for its copies in flight and returns.
+#pragma once
+#include "fwi_step.cuh"
+
+namespace fwi {
+
+typedef unsigned long long u64;
+
+// ------------------------------------------------------------ packed f32x2 arithmetic
+__device__ __forceinline__ u64 pk(float a, float b)
+{
+    u64 r;
+    asm("mov.b64 %0, {%1, %2};" : "=l"(r) : "f"(a), "f"(b));
+    return r;
+}
+__device__ __forceinline__ float2 upk(u64 r)
+{
+    float a, b;
+    asm("mov.b64 {%0, %1}, %2;" : "=f"(a), "=f"(b) : "l"(r));
+    return make_float2(a, b);
+}
+__device__ __forceinline__ u64 add2(u64 a, u64 b)
+{
+    u64 d;
+    asm("add.rn.f32x2 %0, %1, %2;" : "=l"(d) : "l"(a), "l"(b));
+    return d;
+}
+__device__ __forceinline__ u64 sub2(u64 a, u64 b)
+{
+    u64 d;
+    asm("sub.rn.f32x2 %0, %1, %2;" : "=l"(d) : "l"(a), "l"(b));
+    return d;
+}
+__device__ __forceinline__ u64 mul2(u64 a, u64 b)
+{
+    u64 d;
+    asm("mul.rn.f32x2 %0, %1, %2;" : "=l"(d) : "l"(a), "l"(b));
+    return d;
+}
+__device__ __forceinline__ u64 fma2(u64 a, u64 b, u64 c)
+{
+    u64 d;
+    asm("fma.rn.f32x2 %0, %1, %2, %3;" : "=l"(d) : "l"(a), "l"(b), "l"(c));
+    return d;
+}
+
+// stencil constants (propagation.h) and grid spacings as packed pairs.  nz holds -0.0 in
+// both halves, loaded at run time: the exact path forms every product as fma(a, b, nz),
+// which is round(a*b) bit for bit.  A plain packed multiply would be fused by the
+// compiler into a following packed add (one rounding instead of two) although both carry
+// .rn; an addend it cannot see is -0 keeps each product a separate, rounded step.
+struct PkConst {
+    u64 C1, C2, C3, D0, D1, D2, D3, idx, idz, idxx, idzz, nz;
+};
+
+// two vertically adjacent cells of one column: propagation.c:13-74 with each product and
+// sum rounded on its own, in the reference's order
+template <int MATH>
+__device__ __forceinline__ u64 cell2(u64 zm3, u64 zm2, u64 zm1, u64 z0, u64 zp1, u64 zp2, u64 zp3, u64 xm3, u64 xm2,
+                                     u64 xm1, u64 xp1, u64 xp2, u64 xp3, u64 c1, u64 c2, u64 ck, u64 irx, u64 irz,
+                                     u64 ir, u64 p0, const PkConst &k)
+{
+    if (MATH == 0) {
+        auto mul = [&](u64 a, u64 b) { return fma2(a, b, k.nz); };
+        const u64 dpdz = mul(add2(add2(mul(k.C1, sub2(zp1, zm1)), mul(k.C2, sub2(zp2, zm2))), mul(k.C3, sub2(zp3, zm3))),
+                             k.idz);
+        const u64 dpdx = mul(add2(add2(mul(k.C1, sub2(xp1, xm1)), mul(k.C2, sub2(xp2, xm2))), mul(k.C3, sub2(xp3, xm3))),
+                             k.idx);
+        const u64 d0 = mul(k.D0, z0);
+        const u64 dzz =
+            mul(add2(add2(add2(d0, mul(k.D1, add2(zp1, zm1))), mul(k.D2, add2(zp2, zm2))), mul(k.D3, add2(zp3, zm3))),
+                k.idzz);
+        const u64 dxx =
+            mul(add2(add2(add2(d0, mul(k.D1, add2(xp1, xm1))), mul(k.D2, add2(xp2, xm2))), mul(k.D3, add2(xp3, xm3))),
+                k.idxx);
+        const u64 lap = add2(add2(mul(irx, dpdx), mul(irz, dpdz)), mul(ir, add2(dxx, dzz)));
+        return add2(add2(mul(c1, z0), mul(c2, p0)), mul(ck, lap));
+    } else {
+        const u64 dpdz = mul2(fma2(k.C3, sub2(zp3, zm3), fma2(k.C2, sub2(zp2, zm2), mul2(k.C1, sub2(zp1, zm1)))), k.idz);
+        const u64 dpdx = mul2(fma2(k.C3, sub2(xp3, xm3), fma2(k.C2, sub2(xp2, xm2), mul2(k.C1, sub2(xp1, xm1)))), k.idx);
+        const u64 d0 = mul2(k.D0, z0);
+        const u64 dzz =
+            mul2(fma2(k.D3, add2(zp3, zm3), fma2(k.D2, add2(zp2, zm2), fma2(k.D1, add2(zp1, zm1), d0))), k.idzz);
+        const u64 dxx =
+            mul2(fma2(k.D3, add2(xp3, xm3), fma2(k.D2, add2(xp2, xm2), fma2(k.D1, add2(xp1, xm1), d0))), k.idxx);
+        const u64 lap = fma2(ir, add2(dxx, dzz), fma2(irz, dpdz, mul2(irx, dpdx)));
+        return fma2(ck, lap, fma2(c2, p0, mul2(c1, z0)));
+    }
+}
+
+__device__ __forceinline__ u64 lo2(const float4 &v) { return pk(v.x, v.y); }
+__device__ __forceinline__ u64 hi2(const float4 &v) { return pk(v.z, v.w); }
+
+// one float4 group (4 cells) as two packed pairs; lo/cq/hi: groups g-1, g, g+1 of column x;
+// xn: column x-3, x-2, x-1, x+1, x+2, x+3 at group g; cf: c1, c2, coef3*K, irx, irz, ir
+template <int MATH>
+__device__ __forceinline__ float4 group2(const float4 &lo, const float4 &cq, const float4 &hi, const float4 (&xn)[6],
+                                         const float4 (&cf)[6], const float4 &p0, const PkConst &k)
+{
+    const u64 s0 = pk(lo.y, lo.z), s1 = hi2(lo);
+    const u64 s2 = pk(lo.w, cq.x), s3 = lo2(cq), s4 = pk(cq.y, cq.z), s5 = hi2(cq), s6 = pk(cq.w, hi.x);
+    const u64 s7 = lo2(hi), s8 = pk(hi.y, hi.z);
+    const u64 a = cell2<MATH>(s0, s1, s2, s3, s4, s5, s6, lo2(xn[0]), lo2(xn[1]), lo2(xn[2]), lo2(xn[3]), lo2(xn[4]),
+                              lo2(xn[5]), lo2(cf[0]), lo2(cf[1]), lo2(cf[2]), lo2(cf[3]), lo2(cf[4]), lo2(cf[5]), lo2(p0),
+                              k);
+    const u64 b = cell2<MATH>(s2, s3, s4, s5, s6, s7, s8, hi2(xn[0]), hi2(xn[1]), hi2(xn[2]), hi2(xn[3]), hi2(xn[4]),
+                              hi2(xn[5]), hi2(cf[0]), hi2(cf[1]), hi2(cf[2]), hi2(cf[3]), hi2(cf[4]), hi2(cf[5]), hi2(p0),
+                              k);
+    const float2 ra = upk(a), rb = upk(b);
+    return make_float4(ra.x, ra.y, rb.x, rb.y);
+}
+
+// ------------------------------------------------------------ TMA and mbarrier
+__device__ __forceinline__ unsigned smem_u32(const void *p) { return (unsigned)__cvta_generic_to_shared(p); }
+__device__ __forceinline__ u64 global_ns()
+{
+    u64 t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    return t;
+}
+__device__ __forceinline__ void mbar_init(unsigned bar, unsigned count)
+{
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(bar), "r"(count) : "memory");
+}
+// arrive (the barrier's one arrival) and announce the bytes its copies will deliver
+__device__ __forceinline__ void mbar_arrive_expect(unsigned bar, unsigned bytes)
+{
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar), "r"(bytes) : "memory");
+}
+// announce more bytes without arriving
+__device__ __forceinline__ void mbar_expect(unsigned bar, unsigned bytes)
+{
+    asm volatile("mbarrier.expect_tx.shared::cta.b64 [%0], %1;" ::"r"(bar), "r"(bytes) : "memory");
+}
+// waits for the phase of the given parity to complete; false after two seconds
+__device__ __forceinline__ bool mbar_wait(unsigned bar, unsigned parity)
+{
+    const u64 t0 = global_ns();
+    for (;;) {
+        unsigned done;
+        asm volatile(
+            "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"
+            : "=r"(done)
+            : "r"(bar), "r"(parity)
+            : "memory");
+        if (done) return true;
+        if (global_ns() - t0 > 2000000000ull) return false;
+    }
+}
+// tensor map written by the host through the generic proxy, read by the copy engine
+__device__ __forceinline__ void tmap_acquire(const CUtensorMap *m)
+{
+    asm volatile("fence.proxy.tensormap::generic.acquire.gpu [%0], 128;" ::"l"(m) : "memory");
+}
+// 3-D tile copy global -> this CTA's shared memory, completing on bar (no multicast)
+__device__ __forceinline__ void tma_load3(unsigned dst, const CUtensorMap *m, int c0, int c1, int c2, unsigned bar)
+{
+    asm volatile(
+        "cp.async.bulk.tensor.3d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4}], "
+        "[%5];" ::"r"(dst),
+        "l"(m), "r"(c0), "r"(c1), "r"(c2), "r"(bar)
+        : "memory");
+}
+
+// ------------------------------------------------------------ tile geometry
+constexpr int TILE_CH_MAX = 32;  // most shots one block walks
+__host__ __device__ constexpr int round128(int b) { return (b + 127) / 128 * 128; }
+
+template <int TX>
+struct TileGeom {
+    static constexpr int ZP = 4 * (TG + 2);  // p1 tile rows: groups G0-1 .. G0+TG
+    static constexpr int ZC = 4 * TG;        // rows of the computed tile
+    static constexpr int XP = TX + 6;        // p1 tile columns: X0-3 .. X0+TX+2
+    static constexpr int P1_BYTES = ZP * XP * 4;
+    static constexpr int P0_BYTES = ZC * TX * 4;
+    static constexpr int CF_BYTES = 6 * ZC * TX * 4;
+    static constexpr int P0_OFF = round128(P1_BYTES);
+    static constexpr int STAGE = P0_OFF + round128(P0_BYTES);
+    static constexpr int ST_OFF = round128(CF_BYTES);
+    static constexpr int smem(int nst) { return ST_OFF + nst * STAGE; }
+};
+// tile width -> index of the tensor maps in ShotDesc
+template <int TX>
+constexpr int tile_w() { return TX == 16 ? 1 : 0; }
+
+// grid: x = column tile (plus one receiver-sampling index), y = 2 * shot chunk + program
+// item, z = tile of TG z-groups.  block = TG x TX threads.  Dynamic shared memory:
+// TileGeom<TX>::smem(NST).
+template <int TX, int NST, int MATH>
+__global__ void __launch_bounds__(TG *TX) k_tile(const ShotDesc *__restrict__ shots, const int4 *__restrict__ prog,
+                                                 int L, int shot_base, int nshot, int chunk, int *err)
+{
+    using Geo = TileGeom<TX>;
+    constexpr int NT = TG * TX, W = tile_w<TX>();
+    extern __shared__ __align__(128) unsigned char smem[];
+    __shared__ __align__(8) unsigned long long bar[NST];
+    __shared__ float *s_out[TILE_CH_MAX];
+    __shared__ const float *s_u[TILE_CH_MAX];
+    __shared__ double s_srcd[TILE_CH_MAX];
+    __shared__ float s_srcf[TILE_CH_MAX];
+    __shared__ int s_isx[TILE_CH_MAX], s_isz[TILE_CH_MAX], s_rz0[TILE_CH_MAX], s_rz1[TILE_CH_MAX];
+    __shared__ int s_fi[2];  // frames of p1 and p0 (the same for every shot of the chunk)
+
+    const int4 pw = prog[L];
+    const int kind = (blockIdx.y & 1) ? pw.z : pw.x;
+    const int it = (blockIdx.y & 1) ? pw.w : pw.y;
+    if (kind == K_NONE) return;
+    const int cb = shot_base + (blockIdx.y >> 1) * chunk;
+    const int n = min(chunk, shot_base + nshot - cb);
+    if (n <= 0) return;
+    const ShotDesc &A = shots[cb];  // geometry and coefficients of the chunk
+    const int Nx = A.Nx, pml = A.pml, G = A.G, Nz = A.Nz;
+    const int ntx = (Nx + TX - 1) / TX;
+    const bool fwd = kind == K_FWD0 || kind == K_FWD1;
+    const int tid = threadIdx.y * TG + threadIdx.x;
+
+    // ---- the receiver-sampling block: p1 is read-only during this launch
+    if ((int)blockIdx.x >= ntx) {
+        if (!fwd || it % A.sr != 0 || (int)blockIdx.x > ntx || blockIdx.z != 0) return;
+        for (int s = 0; s < n; ++s) {
+            const ShotDesc &D = shots[cb + s];
+            const float *p1 = fwd_buf(D, it, kind == K_FWD1);
+            float *tr = D.traces_t + (long long)(it / D.sr) * D.ntr;
+            for (int r = tid; r < D.ntr; r += NT) tr[r] = p1[D.rec_off[r]];
+        }
+        return;
+    }
+
+    // ---- per-shot scalars of the chunk (frame indices need divisions: once per block)
+    if (tid < n) {
+        const ShotDesc &D = shots[cb + tid];
+        int i1, i0, io, iu = -1;
+        if (fwd) {
+            const bool keep = kind == K_FWD1;
+            i1 = fwd_idx(D, it, keep); i0 = fwd_idx(D, it - 1, keep); io = fwd_idx(D, it + 1, keep);
+        } else if (kind == K_REP) {
+            i1 = rep_idx(D, it); i0 = rep_idx(D, it - 1); io = rep_idx(D, it + 1);
+        } else {
+            i1 = adj_idx(D, it); i0 = adj_idx(D, it + 1); io = adj_idx(D, it - 1);
+            if (it % MST == 0) iu = img_idx(D, it);
+        }
+        s_out[tid] = frame_ptr(D, io);
+        s_u[tid] = iu >= 0 ? frame_ptr(D, iu) : nullptr;
+        s_isx[tid] = D.isx;
+        s_isz[tid] = D.isz;
+        s_srcd[tid] = fwd ? D.srcd[it] : 0.0;
+        s_srcf[tid] = kind == K_REP ? D.srcf[it] : 0.0f;
+        s_rz0[tid] = D.rz0;
+        s_rz1[tid] = D.rz1;
+        if (tid == 0) {
+            s_fi[0] = i1;
+            s_fi[1] = i0;
+        }
+    }
+    const int X0 = blockIdx.x * TX, G0 = blockIdx.z * TG;
+    unsigned char *st_base = smem + Geo::ST_OFF;
+    // stage j of shot s: p1 rows 4*(G0-1).., columns X0-3..; p0 rows 4*G0.., columns X0..
+    auto issue = [&](int j, int s) {
+        const ShotDesc &D = shots[cb + s];
+        tmap_acquire(&D.tm_p1[W]);
+        tmap_acquire(&D.tm_p0[W]);
+        const unsigned b = smem_u32(&bar[j]);
+        mbar_arrive_expect(b, Geo::P1_BYTES + Geo::P0_BYTES);
+        unsigned char *stg = st_base + j * Geo::STAGE;
+        tma_load3(smem_u32(stg), &D.tm_p1[W], 4 * (G0 - 1), X0 - 3, s_fi[0], b);
+        tma_load3(smem_u32(stg + Geo::P0_OFF), &D.tm_p0[W], 4 * G0, X0, s_fi[1], b);
+    };
+    if (tid == 0) {
+        for (int j = 0; j < NST; ++j) mbar_init(smem_u32(&bar[j]), 1);
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    __syncthreads();  // barriers and the per-shot scalars
+    if (tid == 0) {
+        // the coefficient tiles join the first stage's transaction
+        tmap_acquire(&A.tm_cf[W]);
+        mbar_expect(smem_u32(&bar[0]), Geo::CF_BYTES);
+        tma_load3(smem_u32(smem), &A.tm_cf[W], 4 * G0, X0, 0, smem_u32(&bar[0]));
+        for (int j = 0; j < NST && j < n; ++j) issue(j, j);
+    }
+
+    // ---- per-thread constants
+    const int g = G0 + threadIdx.x, k = threadIdx.y;
+    const int x = X0 + k, z0 = 4 * g;
+    const bool mine = g < G && x < Nx;
+    const int zlo = A.izStart, zhi = Nz - 4;
+    const bool zfd = z0 + 3 >= zlo && z0 <= zhi;
+    const bool zpart = z0 < zlo || z0 + 3 > zhi;  // group straddles the edge of the updated rows
+    const bool any = mine && zfd && x >= 3 && x <= Nx - 4;
+    const bool fs_top = A.fs && mine && z0 <= 2 * pml;  // the free-surface row or the rows it mirrors
+    const int jpml = (pml >= z0 && pml < z0 + 4) ? pml - z0 : -1;
+    const bool inject = kind == K_ADJ && it >= 1;
+    const bool hess = kind == K_FWD1 && A.hessian && (it % MST == 0);
+    const bool image = kind == K_ADJ && (it % MST == 0);
+    const bool acc_here = mine && (hess || image) && z0 + 3 >= pml && z0 < pml + A.nz && x >= pml && x < pml + A.nxx;
+    const long long colx = (long long)x * A.ld, col = colx + z0;
+    const float invdx = A.invdx, invdz = A.invdz, invdtdt = A.invdtdt;
+    PkConst K;
+    K.C1 = pk(0.77793115f, 0.77793115f);
+    K.C2 = pk(-0.17388691f, -0.17388691f);
+    K.C3 = pk(0.02338713f, 0.02338713f);
+    K.D0 = pk(-2.8215452f, -2.8215452f);
+    K.D1 = pk(1.57663238f, 1.57663238f);
+    K.D2 = pk(-0.18347238f, -0.18347238f);
+    K.D3 = pk(0.01761260f, 0.01761260f);
+    K.idx = pk(invdx, invdx);
+    K.idz = pk(invdz, invdz);
+    K.idxx = pk(A.invdxdx, A.invdxdx);
+    K.idzz = pk(A.invdzdz, A.invdzdz);
+    K.nz = pk(A.negzero, A.negzero);
+    const float4 zero4 = make_float4(0.f, 0.f, 0.f, 0.f);
+    const float4(*scf)[TX][TG] = reinterpret_cast<const float4(*)[TX][TG]>(smem);
+    float4 cf[6];
+
+    int i = 0;
+    for (; i < n; ++i) {
+        const int st = i % NST;
+        const int ok = __syncthreads_and(tid == 0 ? (int)mbar_wait(smem_u32(&bar[st]), (i / NST) & 1) : 1);
+        if (!ok) break;
+        // every thread is past shot i-1: its stage takes shot i-1+NST
+        if (tid == 0 && i >= 1 && i - 1 + NST < n) issue((i - 1) % NST, i - 1 + NST);
+        if (i == 0) {
+#pragma unroll
+            for (int f = 0; f < 6; ++f) cf[f] = scf[f][k][threadIdx.x];
+        }
+        if (!mine) continue;
+        const unsigned char *stg = st_base + st * Geo::STAGE;
+        const float4(*sp1)[TG + 2] = reinterpret_cast<const float4(*)[TG + 2]>(stg);
+        const float4(*sp0)[TG] = reinterpret_cast<const float4(*)[TG]>(stg + Geo::P0_OFF);
+        const int cx = k + 3, cg = threadIdx.x + 1;
+        const float4 cq = sp1[cx][cg];
+        const float4 p0 = sp0[k][threadIdx.x];
+        float4 v = zero4;
+        if (any) {
+            const float4 xn[6] = {sp1[cx - 3][cg], sp1[cx - 2][cg], sp1[cx - 1][cg],
+                                  sp1[cx + 1][cg], sp1[cx + 2][cg], sp1[cx + 3][cg]};
+            v = group2<MATH>(sp1[cx][cg - 1], cq, sp1[cx][cg + 1], xn, cf, p0, K);
+            if (zpart) {
+                if (z0 < zlo || z0 > zhi) v.x = 0.f;
+                if (z0 + 1 < zlo || z0 + 1 > zhi) v.y = 0.f;
+                if (z0 + 2 < zlo || z0 + 2 > zhi) v.z = 0.f;
+                if (z0 + 3 < zlo || z0 + 3 > zhi) v.w = 0.f;
+            }
+        }
+        const int isz = s_isz[i];
+        const bool src_here = x == s_isx[i] && isz >= z0 && isz < z0 + 4;
+        // forward: the source enters before the free surface, in double (propagation.c:558-564)
+        if (fwd && src_here) setc(v, isz - z0, (float)__dadd_rn((double)comp(v, isz - z0), s_srcd[i]));
+        float4 mir = zero4;
+        if (fs_top) {
+            if (jpml >= 0) setc(v, jpml, -0.0f);
+            mir = make_float4(-v.x, -v.y, -v.z, -v.w);
+        }
+        // replay: free surface first, then the float source (propagation.c:656-662)
+        if (kind == K_REP && src_here) setc(v, isz - z0, fa(comp(v, isz - z0), s_srcf[i]));
+        if (acc_here) {
+            const ShotDesc &D = shots[cb + i];
+            const float4 uu = image ? ldg4(s_u[i] + col) : zero4;
+            double2 *acc = reinterpret_cast<double2 *>((image ? D.Gacc : D.H) + col);
+            double2 a0 = acc[0], a1 = acc[1];
+            double a[4] = {a0.x, a0.y, a1.x, a1.y};
+#pragma unroll
+            for (int j = 0; j < 4; ++j) {
+                const int z = z0 + j;
+                if (z < pml || z >= pml + D.nz) continue;
+                float t = fm(fa(fs_(comp(v, j), fm(2.0f, comp(cq, j))), comp(p0, j)), invdtdt);
+                float w = image ? fm(t, comp(uu, j)) : fm(t, t);
+                a[j] = __dadd_rn(a[j], (double)w);
+            }
+            acc[0] = make_double2(a[0], a[1]);
+            acc[1] = make_double2(a[2], a[3]);
+        }
+        if (inject && z0 + 3 >= s_rz0[i] && z0 <= s_rz1[i]) {
+            const ShotDesc &D = shots[cb + i];
+            const int e0 = __ldg(D.colptr + x), e1 = __ldg(D.colptr + x + 1);
+            const float *arow = D.adj_t + (long long)(it - 1) * D.ntr;
+            for (int e = e0; e < e1; ++e) {
+                const int2 r = __ldg(D.rec + e);
+                if (r.x < z0 || r.x >= z0 + 4) continue;
+                const int j = r.x - z0;
+                float a = fm(fm(fm(fm(fm(__ldg(arow + r.y), __ldg(D.recK + e)), D.dt), D.dt), invdx), invdz);
+                setc(v, j, fs_(comp(v, j), a));
+            }
+        }
+        float *out = s_out[i];
+        if (!fs_top || z0 >= pml) {
+            *reinterpret_cast<float4 *>(out + col) = v;
+        } else {
+#pragma unroll
+            for (int j = 0; j < 4; ++j)
+                if (z0 + j >= pml) out[col + j] = comp(v, j);
+        }
+        if (fs_top) {
+#pragma unroll
+            for (int j = 0; j < 4; ++j) {
+                const int z = z0 + j;
+                if (z > pml && z <= 2 * pml) out[colx + 2 * pml - z] = comp(mir, j);
+            }
+        }
+    }
+    if (i < n && tid == 0) {
+        // a copy did not land in time: report it and let the copies in flight finish
+        atomicExch(err, 1);
+        const int last = min(n, (i > 0 ? i - 1 : 0) + NST);
+        for (int j = i; j < last; ++j) mbar_wait(smem_u32(&bar[j % NST]), (j / NST) & 1);
+    }
+}
+
+}  // namespace fwi
