@@ -133,6 +133,15 @@ struct fwi_ctx {
     fwi_stats stats{};
     int math = 0;  // 0: bit-exact arithmetic, 1: contracted multiply-adds
     int *d_err = nullptr;  // set by a step kernel whose tile copy did not complete
+    // frame pools: the frame blocks of a shot group, consecutive (key: first shot of the
+    // group on the batched path, -1 for the plain path's single shot)
+    struct Pool {
+        float *p = nullptr;
+        size_t bytes = 0;
+        int nfr = 0, ng = 0;
+        long long frame = 0;
+    };
+    std::map<int, Pool> pools;
     long long launches = 0;
     double last_obj = 0.0;
 };
@@ -172,6 +181,8 @@ static void free_runs(fwi_ctx *c)
     drop_graphs(c);
     for (auto &r : c->runs) free_run(c, r.get());
     c->runs.clear();
+    for (auto &kv : c->pools) dfree(c, kv.second.p, kv.second.bytes);
+    c->pools.clear();
 }
 
 extern "C" int fwi_ctx_create(fwi_ctx **out, int device, size_t budget)
@@ -424,30 +435,69 @@ static PFN_cuTensorMapEncodeTiled_v12000 tensor_map_encoder()
     return fn;
 }
 
-// 3-D float map {d0 (z, contiguous), d1 (x), d2 (frames or planes)}, box {b0, b1, b2};
+// float tensor map of rank 3 or 4: dims[0] contiguous (z), then x, frames or planes, shots;
 // out-of-range elements of a box read as zero
-static int encode_map(CUtensorMap *m, const float *base, int d0, int d1, int d2, int b0, int b1, int b2)
+static int encode_map(CUtensorMap *m, const float *base, int rank, const long long *dims, const int *box)
 {
     PFN_cuTensorMapEncodeTiled_v12000 enc = tensor_map_encoder();
     if (!enc) return fail(FWI_ERR_CUDA, "cuTensorMapEncodeTiled is not available from the driver");
-    const cuuint64_t dims[3] = {(cuuint64_t)d0, (cuuint64_t)d1, (cuuint64_t)d2};
-    const cuuint64_t strides[2] = {(cuuint64_t)d0 * 4, (cuuint64_t)d0 * d1 * 4};
-    const cuuint32_t box[3] = {(cuuint32_t)b0, (cuuint32_t)b1, (cuuint32_t)b2}, es[3] = {1, 1, 1};
-    CUresult r = enc(m, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 3, (void *)base, dims, strides, box, es,
+    cuuint64_t gd[4], gs[3];
+    cuuint32_t bx[4], es[4] = {1, 1, 1, 1};
+    unsigned long long stride = 4;
+    for (int i = 0; i < rank; i++) {
+        gd[i] = (cuuint64_t)dims[i];
+        bx[i] = (cuuint32_t)box[i];
+        if (i > 0) gs[i - 1] = stride;
+        stride *= (unsigned long long)dims[i];
+    }
+    CUresult r = enc(m, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, (cuuint32_t)rank, (void *)base, gd, gs, bx, es,
                      CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
                      CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
     if (r != CUDA_SUCCESS) return fail(FWI_ERR_CUDA, "cuTensorMapEncodeTiled failed (%d)", (int)r);
     return FWI_OK;
 }
 
+// the three maps of a launch over nshot consecutive frame blocks starting at d0's
 template <int TX>
-static int encode_tile_maps(ShotDesc &d, const float *coef)
+static int encode_group_maps(const ShotDesc &d0, int nshot, const float *coef, CUtensorMap *p1, CUtensorMap *p0,
+                             CUtensorMap *cf)
 {
     using Geo = TileGeom<TX>;
-    constexpr int w = tile_w<TX>();
-    TRY(encode_map(&d.tm_p1[w], d.frames, d.ld, d.Nx, d.nfr, Geo::ZP, Geo::XP, 1));
-    TRY(encode_map(&d.tm_p0[w], d.frames, d.ld, d.Nx, d.nfr, Geo::ZC, TX, 1));
-    TRY(encode_map(&d.tm_cf[w], coef, d.ld, d.Nx, 6, Geo::ZC, TX, 6));
+    const long long pd[4] = {d0.ld, d0.Nx, d0.nfr, nshot}, cd[3] = {d0.ld, d0.Nx, 6};
+    const int b1[4] = {Geo::ZP, Geo::XP, 1, 1}, b0[4] = {Geo::ZC, TX, 1, 1}, bc[3] = {Geo::ZC, TX, 6};
+    TRY(encode_map(p1, d0.frames, 4, pd, b1));
+    TRY(encode_map(p0, d0.frames, 4, pd, b0));
+    TRY(encode_map(cf, coef, 3, cd, bc));
+    return FWI_OK;
+}
+
+// frame blocks of a group of runs, consecutive in one pool; a new pool or a new layout
+// invalidates the captured launches (their tensor maps hold the old one)
+static int assign_pool(fwi_ctx *c, int key, const std::vector<ShotRun *> &rs)
+{
+    const ShotDesc &d0 = rs[0]->d;
+    const int ng = (int)rs.size();
+    const size_t per = (size_t)d0.nfr * (size_t)d0.frame;
+    const size_t need = per * ng * 4;
+    fwi_ctx::Pool &pl = c->pools[key];
+    if (pl.bytes < need || pl.nfr != d0.nfr || pl.ng != ng || pl.frame != d0.frame) {
+        drop_graphs(c);
+        if (pl.bytes < need) {
+            dfree(c, pl.p, pl.bytes);
+            pl.p = nullptr;
+            pl.bytes = 0;
+            TRY(dmalloc(c, (void **)&pl.p, need));
+            pl.bytes = need;
+        }
+        pl.nfr = d0.nfr;
+        pl.ng = ng;
+        pl.frame = d0.frame;
+    }
+    for (int i = 0; i < ng; i++) {
+        if (rs[i]->d.nfr != d0.nfr || rs[i]->d.frame != d0.frame)
+            return fail(FWI_ERR_STATE, "shots of one group differ in frame layout");
+        rs[i]->d.frames = pl.p + per * i;
+    }
     return FWI_OK;
 }
 
@@ -493,7 +543,7 @@ static int prepare_run(fwi_ctx *c, ShotRun *r, int shot, bool gradient)
         TRY(ralloc(c, r, &q, (size_t)ntr * 4)); d.rec_off = (int *)q;
         TRY(ralloc(c, r, &q, (size_t)s.ns * ntr * 4)); d.traces_t = (float *)q;
         d.nfr = gradient ? nframes_gradient(d.K, d.S5) : 3;
-        TRY(ralloc(c, r, &q, (size_t)d.nfr * fr * 4)); d.frames = (float *)q;
+        d.frames = nullptr;  // in the group's pool (assign_pool)
         d.H = d.Gacc = nullptr;
         d.adj_t = nullptr;
         if (gradient) {
@@ -547,8 +597,6 @@ static int prepare_run(fwi_ctx *c, ShotRun *r, int shot, bool gradient)
         d.rz0 = std::min(d.rz0, sh.igz[i] + c->pml);
         d.rz1 = std::max(d.rz1, sh.igz[i] + c->pml);
     }
-    TRY(encode_tile_maps<8>(d, p->d_coef));
-    TRY(encode_tile_maps<16>(d, p->d_coef));
     CK(cudaMemcpyAsync((void *)d.srcd, sd.data(), nt * 8, cudaMemcpyHostToDevice, c->stream));
     CK(cudaMemcpyAsync((void *)d.srcf, sf.data(), nt * 4, cudaMemcpyHostToDevice, c->stream));
     CK(cudaMemcpyAsync((void *)d.colptr, colptr.data(), (d.Nx + 1) * 4, cudaMemcpyHostToDevice, c->stream));
@@ -704,7 +752,8 @@ static LaunchCfg pick_launch(int Nx, int nshot, bool batched, int math)
     return L;
 }
 
-typedef void (*TileFn)(const ShotDesc *, const int4 *, int, int, int, int, int *);
+typedef void (*TileFn)(const CUtensorMap, const CUtensorMap, const CUtensorMap, const ShotDesc *, const int4 *, int,
+                       int, int, int, int *);
 
 template <int TX, int NST, int MATH>
 static TileFn tile_fn()
@@ -726,28 +775,28 @@ static TileFn tile_fn_nst(int nst)
     return nst == 2 ? tile_fn<TX, 2, MATH>() : nst == 4 ? tile_fn<TX, 4, MATH>() : tile_fn<TX, 3, MATH>();
 }
 
-// shots per block: the most (up to TILE_CH_MAX) whose grid still fills the last wave of
-// resident blocks about as well as the best choice does
+// shots per block: split the group into equal chunks (at most TILE_CH_MAX shots each) and
+// take the fewest chunks whose grid fills its last wave of resident blocks about as well
+// as the best split does
 static int pick_chunk(int tiles, int nshot, int resident)
 {
     const int slots = 148 * resident;
-    auto fill = [&](int ch) {
-        const long long blocks = (long long)tiles * ((nshot + ch - 1) / ch);
+    auto fill = [&](int nch) {
+        const long long blocks = (long long)tiles * nch;
         const long long waves = (blocks + slots - 1) / slots;
         return (double)blocks / (double)(waves * slots);
     };
+    const int nmin = (nshot + TILE_CH_MAX - 1) / TILE_CH_MAX;
     double best = 0.0;
-    for (int ch = 1; ch <= std::min(nshot, TILE_CH_MAX); ch++) best = std::max(best, fill(ch));
-    int pick = 1;
-    for (int ch = 1; ch <= std::min(nshot, TILE_CH_MAX); ch++)
-        if (fill(ch) >= 0.9 * best) pick = ch;
-    return pick;
+    for (int nch = nmin; nch <= nshot; nch++) best = std::max(best, fill(nch));
+    for (int nch = nmin; nch <= nshot; nch++)
+        if (fill(nch) >= 0.9 * best) return (nshot + nch - 1) / nch;
+    return 1;
 }
 
-static int launch_steps(fwi_ctx *c, const Program *prog, int shot_base, int nshot, int prog_stride, const Plan *p,
-                        bool batched)
+static int launch_steps(fwi_ctx *c, const Program *prog, int shot_base, int nshot, const ShotRun *r0, bool batched)
 {
-    (void)prog_stride;
+    const Plan *p = r0->plan;
     const int zt = (p->G + TG - 1) / TG;
     const int n = (int)prog->items.size();
     const char *ke = getenv("FWI_KERNEL");  // "step": the cp.async kernel, kept for comparison
@@ -766,7 +815,7 @@ static int launch_steps(fwi_ctx *c, const Program *prog, int shot_base, int nsho
     }
     int tx = batched ? 16 : 8;
     if (const char *e = getenv("FWI_TX")) tx = atoi(e) == 8 ? 8 : 16;
-    int nst = tx == 16 ? 3 : 4;
+    int nst = 4;
     if (const char *e = getenv("FWI_NST")) nst = std::min(4, std::max(2, atoi(e)));
     const int ntx = (p->Nx + tx - 1) / tx;
     int chunk = pick_chunk(ntx * zt, nshot, tx == 16 ? 2 : 4);
@@ -776,10 +825,14 @@ static int launch_steps(fwi_ctx *c, const Program *prog, int shot_base, int nsho
     const int smem = tx == 16 ? TileGeom<16>::smem(nst) : TileGeom<8>::smem(nst);
     const int nchunks = (nshot + chunk - 1) / chunk;
     dim3 grid(ntx + 1, 2 * nchunks, zt);
+    CUtensorMap m1, m0, mc;
+    if (tx == 16) TRY(encode_group_maps<16>(r0->d, nshot, p->d_coef, &m1, &m0, &mc));
+    else TRY(encode_group_maps<8>(r0->d, nshot, p->d_coef, &m1, &m0, &mc));
     for (int L = 0; L < n; L++) {
         const int4 &pw = prog->items[L];
         if (pw.x == K_NONE && pw.z == K_NONE) continue;
-        fn<<<grid, dim3(TG, tx), smem, c->stream>>>(c->d_desc, prog->d, L, shot_base, nshot, chunk, c->d_err);
+        fn<<<grid, dim3(TG, tx + 2), smem, c->stream>>>(m1, m0, mc, c->d_desc, prog->d, L, shot_base, nshot, chunk,
+                                                         c->d_err);
         c->launches++;
     }
     CK(cudaGetLastError());
@@ -1033,17 +1086,17 @@ static int adj_init(fwi_ctx *c, const std::vector<ShotRun *> &rs, int shot_base)
 
 // run a program over a group of shots, through a cached CUDA graph on the batched path
 static int run_program(fwi_ctx *c, const std::string &key, const Program *prog, int shot_base, int nshot,
-                       const Plan *p, bool batched)
+                       const ShotRun *r0, bool batched)
 {
-    if (!batched) return launch_steps(c, prog, shot_base, nshot, 0, p, false);
+    if (!batched) return launch_steps(c, prog, shot_base, nshot, r0, false);
     const char *ge = getenv("FWI_GRAPH");  // FWI_GRAPH=0: issue the launches directly (profilers, debugging)
-    if (ge && ge[0] == '0') return launch_steps(c, prog, shot_base, nshot, 0, p, true);
+    if (ge && ge[0] == '0') return launch_steps(c, prog, shot_base, nshot, r0, true);
     auto it = c->graphs.find(key);
     if (it == c->graphs.end()) {
         cudaGraph_t g;
         CK(cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal));
         long long before = c->launches;
-        int rc = launch_steps(c, prog, shot_base, nshot, 0, p, true);
+        int rc = launch_steps(c, prog, shot_base, nshot, r0, true);
         cudaError_t e = cudaStreamEndCapture(c->stream, &g);
         if (rc != FWI_OK) return rc;
         if (e != cudaSuccess) return fail(FWI_ERR_CUDA, "graph capture: %s", cudaGetErrorString(e));
@@ -1068,7 +1121,7 @@ static int run_forward_group(fwi_ctx *c, std::vector<ShotRun *> &rs, int problem
     Program *prog;
     TRY(get_program(c, "fwd0", program_forward(c->nt, K_FWD0), &prog));
     for (ShotRun *r : rs) TRY(zero_initial(c, r, false));
-    TRY(run_program(c, "fwd0/" + gkey, prog, shot_base, (int)rs.size(), rs[0]->plan, batched));
+    TRY(run_program(c, "fwd0/" + gkey, prog, shot_base, (int)rs.size(), rs[0], batched));
     if (problem == 2) {
         if (filter == 0 || filter == 1) return fail(FWI_ERR_UNSUPPORTED, "residual filter %d (FFT) is not built", filter);
         for (ShotRun *r : rs) TRY(prepare_taper(c, r, freq));
@@ -1084,7 +1137,7 @@ static int grad_forward(fwi_ctx *c, std::vector<ShotRun *> &rs, int precondition
     Program *pf;
     TRY(get_program(c, "fwd1", program_forward(c->nt, K_FWD1), &pf));
     for (ShotRun *r : rs) TRY(zero_initial(c, r, true));
-    TRY(run_program(c, "fwd1/" + gkey, pf, shot_base, (int)rs.size(), rs[0]->plan, batched));
+    TRY(run_program(c, "fwd1/" + gkey, pf, shot_base, (int)rs.size(), rs[0], batched));
     if (precondition == 1) TRY(finalize(c, rs, 0));
     return FWI_OK;
 }
@@ -1095,7 +1148,7 @@ static int grad_adjoint(fwi_ctx *c, std::vector<ShotRun *> &rs, bool batched, co
     Program *pa;
     TRY(get_program(c, batched ? "adj/overlap" : "adj/plain", program_adjoint(c->nt, batched), &pa));
     TRY(adj_init(c, rs, shot_base));
-    TRY(run_program(c, std::string(batched ? "adjo/" : "adjp/") + gkey, pa, shot_base, (int)rs.size(), rs[0]->plan,
+    TRY(run_program(c, std::string(batched ? "adjo/" : "adjp/") + gkey, pa, shot_base, (int)rs.size(), rs[0],
                     batched));
     TRY(finalize(c, rs, 1));
     return FWI_OK;
@@ -1144,6 +1197,11 @@ extern "C" int fwi_ctx_run(fwi_ctx *c, int problem, float freq, int filter, int 
             if (groups.empty() || c->runs[i]->plan != c->runs[groups.back().first]->plan) groups.push_back({i, 1});
             else groups.back().second++;
         }
+        for (auto &gr : groups) {
+            std::vector<ShotRun *> rs;
+            for (int i = gr.first; i < gr.first + gr.second; i++) rs.push_back(c->runs[i].get());
+            TRY(assign_pool(c, gr.first, rs));
+        }
         for (int i = 0; i < ns; i++) descs[i] = c->runs[i]->d;
         TRY(upload_descs(c, descs));
         for (auto &gr : groups) {
@@ -1172,6 +1230,7 @@ extern "C" int fwi_ctx_run(fwi_ctx *c, int problem, float freq, int filter, int 
         for (int i = 0; i < ns; i++) {
             TRY(prepare_run(c, r, i, gradient));
             r->d.hessian = gradient && precondition == 1;
+            TRY(assign_pool(c, -1, {r}));
             TRY(upload_descs(c, {r->d}));
             std::vector<ShotRun *> rs = {r};
             if (gradient) {
@@ -1382,7 +1441,7 @@ extern "C" int fwi_iso_acoustic2d_propagation_engine(Record2D *r, Acoustic2dChec
         TRY(grad_adjoint(c, rs, false, "", 0));
         CK(cudaMemcpyAsync(grad[0], sr->d_gshot, (size_t)nx * nz * 4, cudaMemcpyDeviceToHost, c->stream));
         CK(cudaStreamSynchronize(c->stream));
-        return FWI_OK;
+        return check_kernel_error(c);
     }
     TRY(fwi_ctx_set_model(c, vpm[0], rhom[0], nz, nx, dx, dz, dt, nt, pml, fs));
     TRY(fwi_ctx_set_shots(c, &s, 1));
@@ -1399,6 +1458,7 @@ extern "C" int fwi_iso_acoustic2d_propagation_engine(Record2D *r, Acoustic2dChec
     ShotRun *sr = c->runs[0].get();
     TRY(prepare_run(c, sr, 0, true));
     sr->d.hessian = precondition == 1;
+    TRY(assign_pool(c, -1, {sr}));
     TRY(upload_descs(c, {sr->d}));
     std::vector<ShotRun *> rs = {sr};
     TRY(grad_forward(c, rs, precondition, false, "", 0));
@@ -1407,6 +1467,7 @@ extern "C" int fwi_iso_acoustic2d_propagation_engine(Record2D *r, Acoustic2dChec
     if (precondition == 1 && grad)
         CK(cudaMemcpyAsync(grad[0], sr->d_hshot, (size_t)nx * nz * 4, cudaMemcpyDeviceToHost, c->stream));
     CK(cudaStreamSynchronize(c->stream));
+    TRY(check_kernel_error(c));
     k->forward_done = true;
     return FWI_OK;
 }

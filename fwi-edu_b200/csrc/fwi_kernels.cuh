@@ -5,7 +5,6 @@
 // Fields are [Nx][ld] floats, z fastest, ld = Nz rounded up to 4 (16-byte rows).
 #pragma once
 #include <cstdint>
-#include <cuda.h>  // CUtensorMap (the encoded TMA descriptor type; no driver call is made here)
 #include <cuda_runtime.h>
 
 namespace fwi {
@@ -41,7 +40,8 @@ struct ShotDesc {
     const int *rec_off;    // per receiver (trace order): padded cell offset X*ld + Z
     float *traces_t;       // [ns][ntr] samples of the forward pass
     const float *adj_t;    // [nt][ntr] adjoint source
-    // wavefield storage: one block of nfr frames of Nx*ld floats per shot, laid out as
+    // wavefield storage: one block of nfr frames of Nx*ld floats per shot (the blocks of a
+    // shot group are consecutive in one pool, so one tensor map covers the group), laid out as
     // F_FWD (3 forward frames), F_ADJ (3 adjoint), F_REP (3 replay), F_CK (2(K+1) checkpoint
     // slots: slot 0 = u(-1), 2k+1 = u(kd), 2k = u(kd-1)), then 2*S5 replayed frames kept for
     // imaging (t % 5 == 0), double-buffered by segment.  A forward-only run has nfr = 3.
@@ -50,10 +50,6 @@ struct ShotDesc {
     double *H, *Gacc;      // [Nx][ld] FP64 accumulators (pseudo-Hessian, gradient)
     long long frame;       // Nx*ld
     int rz0, rz1;          // padded depth range of this shot's receivers
-    // TMA descriptors, per tile width w (0: 8 columns, 1: 16 columns): the p1 tile with its
-    // halo and the p0 tile over the frame block {ld, Nx, nfr}, and the six coefficient
-    // planes {ld, Nx, 6} of the shot's model window
-    CUtensorMap tm_p1[2], tm_p0[2], tm_cf[2];
 };
 
 // ------------------------------------------------------------ buffer selection

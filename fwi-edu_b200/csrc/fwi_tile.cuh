@@ -1,15 +1,16 @@
 // fwi_tile.cuh -- the TMA-fed time-step kernel.
 //
 // A block owns one tile of the padded grid (TG = 16 float4 z-groups = 64 rows by TX
-// columns, one thread per group and column) and walks a chunk of shots that share
-// the model window.  The shots' fields never pass through registers on their way in:
-// one thread issues, per shot, two tensor copies (cp.async.bulk.tensor) -- the p1 tile
-// with its halo (one group above and below, three columns left and right) and the p0
-// tile -- into a ring of NST shared-memory stages, each completed on its own mbarrier,
-// so the loads of the next NST-1 shots run while the block computes the current one.
-// The six coefficient tiles arrive once per block, by one more tensor copy, and stay in
-// registers for all shots.  Out-of-range parts of a tile (grid edges) are zero-filled by
-// the copy engine.
+// columns, one consumer thread per group and column) and walks a chunk of shots that
+// share the model window.  The shots' fields never pass through registers on their way
+// in: one extra producer warp issues, per shot, two tensor copies (cp.async.bulk.tensor)
+// -- the p1 tile with its halo (one group above and below, three columns left and right)
+// and the p0 tile -- into a ring of NST shared-memory stages.  Each stage has a "full"
+// mbarrier (the copies landed) and an "empty" one (every consumer warp is done with it);
+// consumer warps wait only on the stage they need, so they drift apart by up to NST
+// shots instead of meeting at a block-wide barrier per shot.  The six coefficient tiles
+// arrive once per block, by one more tensor copy, and stay in registers for all shots.
+// Out-of-range parts of a tile (grid edges) are zero-filled by the copy engine.
 //
 // Arithmetic uses the packed f32x2 add/sub/mul of sm_100 on pairs of neighbouring cells,
 // with every operation rounded separately in the reference's association order: the
@@ -28,6 +29,8 @@
 // Every wait is bounded: a tile copy that has not landed after two seconds sets the
 // error word, the block waits (again bounded) for its copies in flight and returns.
 #pragma once
+#include <cuda.h>  // CUtensorMap, the encoded tensor-copy descriptor type
+
 #include "fwi_step.cuh"
 
 namespace fwi {
@@ -160,33 +163,47 @@ __device__ __forceinline__ void mbar_expect(unsigned bar, unsigned bytes)
 {
     asm volatile("mbarrier.expect_tx.shared::cta.b64 [%0], %1;" ::"r"(bar), "r"(bytes) : "memory");
 }
-// waits for the phase of the given parity to complete; false after two seconds
+__device__ __forceinline__ void mbar_arrive(unsigned bar)
+{
+    asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(bar) : "memory");
+}
+__device__ __forceinline__ bool mbar_try(unsigned bar, unsigned parity)
+{
+    unsigned done;
+    asm volatile("{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"
+                 : "=r"(done)
+                 : "r"(bar), "r"(parity)
+                 : "memory");
+    return done != 0;
+}
+// waits for the phase of the given parity to complete; false after two seconds (the clock
+// is read only when the first try finds the phase still open)
 __device__ __forceinline__ bool mbar_wait(unsigned bar, unsigned parity)
 {
+    if (mbar_try(bar, parity)) return true;
     const u64 t0 = global_ns();
     for (;;) {
-        unsigned done;
-        asm volatile(
-            "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"
-            : "=r"(done)
-            : "r"(bar), "r"(parity)
-            : "memory");
-        if (done) return true;
+        if (mbar_try(bar, parity)) return true;
         if (global_ns() - t0 > 2000000000ull) return false;
     }
 }
-// tensor map written by the host through the generic proxy, read by the copy engine
-__device__ __forceinline__ void tmap_acquire(const CUtensorMap *m)
-{
-    asm volatile("fence.proxy.tensormap::generic.acquire.gpu [%0], 128;" ::"l"(m) : "memory");
-}
-// 3-D tile copy global -> this CTA's shared memory, completing on bar (no multicast)
+// tile copies global -> this CTA's shared memory, completing on bar (no multicast); the
+// tensor maps are __grid_constant__ kernel parameters
 __device__ __forceinline__ void tma_load3(unsigned dst, const CUtensorMap *m, int c0, int c1, int c2, unsigned bar)
 {
     asm volatile(
         "cp.async.bulk.tensor.3d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4}], "
         "[%5];" ::"r"(dst),
         "l"(m), "r"(c0), "r"(c1), "r"(c2), "r"(bar)
+        : "memory");
+}
+__device__ __forceinline__ void tma_load4(unsigned dst, const CUtensorMap *m, int c0, int c1, int c2, int c3,
+                                          unsigned bar)
+{
+    asm volatile(
+        "cp.async.bulk.tensor.4d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4, "
+        "%5}], [%6];" ::"r"(dst),
+        "l"(m), "r"(c0), "r"(c1), "r"(c2), "r"(c3), "r"(bar)
         : "memory");
 }
 
@@ -207,21 +224,23 @@ struct TileGeom {
     static constexpr int ST_OFF = round128(CF_BYTES);
     static constexpr int smem(int nst) { return ST_OFF + nst * STAGE; }
 };
-// tile width -> index of the tensor maps in ShotDesc
-template <int TX>
-constexpr int tile_w() { return TX == 16 ? 1 : 0; }
-
 // grid: x = column tile (plus one receiver-sampling index), y = 2 * shot chunk + program
-// item, z = tile of TG z-groups.  block = TG x TX threads.  Dynamic shared memory:
-// TileGeom<TX>::smem(NST).
+// item, z = tile of TG z-groups.  block = TG x (TX + 2) threads: rows 0..TX-1 are the
+// consumers (one z-group of one column each), the last two rows form the producer warp.
+// Dynamic shared memory: TileGeom<TX>::smem(NST).
+// Tensor maps: tm_p1 / tm_p0 describe the group's frame pool {ld, Nx, nfr, nshot} (z
+// contiguous; shot s of the group at index s - shot_base) with boxes {ZP, XP, 1, 1} and
+// {ZC, TX, 1, 1}; tm_cf the six coefficient planes {ld, Nx, 6} with box {ZC, TX, 6}.
 template <int TX, int NST, int MATH>
-__global__ void __launch_bounds__(TG *TX) k_tile(const ShotDesc *__restrict__ shots, const int4 *__restrict__ prog,
-                                                 int L, int shot_base, int nshot, int chunk, int *err)
+__global__ void __launch_bounds__(TG *(TX + 2))
+    k_tile(const __grid_constant__ CUtensorMap tm_p1, const __grid_constant__ CUtensorMap tm_p0,
+           const __grid_constant__ CUtensorMap tm_cf, const ShotDesc *__restrict__ shots, const int4 *__restrict__ prog,
+           int L, int shot_base, int nshot, int chunk, int *err)
 {
     using Geo = TileGeom<TX>;
-    constexpr int NT = TG * TX, W = tile_w<TX>();
+    constexpr int NT = TG * (TX + 2), NW = TG * TX / 32;
     extern __shared__ __align__(128) unsigned char smem[];
-    __shared__ __align__(8) unsigned long long bar[NST];
+    __shared__ __align__(8) unsigned long long full[NST], empty[NST], cfbar;
     __shared__ float *s_out[TILE_CH_MAX];
     __shared__ const float *s_u[TILE_CH_MAX];
     __shared__ double s_srcd[TILE_CH_MAX];
@@ -241,6 +260,7 @@ __global__ void __launch_bounds__(TG *TX) k_tile(const ShotDesc *__restrict__ sh
     const int ntx = (Nx + TX - 1) / TX;
     const bool fwd = kind == K_FWD0 || kind == K_FWD1;
     const int tid = threadIdx.y * TG + threadIdx.x;
+    const int warp = tid >> 5, lane = tid & 31;
 
     // ---- the receiver-sampling block: p1 is read-only during this launch
     if ((int)blockIdx.x >= ntx) {
@@ -280,30 +300,45 @@ __global__ void __launch_bounds__(TG *TX) k_tile(const ShotDesc *__restrict__ sh
             s_fi[1] = i0;
         }
     }
-    const int X0 = blockIdx.x * TX, G0 = blockIdx.z * TG;
-    unsigned char *st_base = smem + Geo::ST_OFF;
-    // stage j of shot s: p1 rows 4*(G0-1).., columns X0-3..; p0 rows 4*G0.., columns X0..
-    auto issue = [&](int j, int s) {
-        const ShotDesc &D = shots[cb + s];
-        tmap_acquire(&D.tm_p1[W]);
-        tmap_acquire(&D.tm_p0[W]);
-        const unsigned b = smem_u32(&bar[j]);
-        mbar_arrive_expect(b, Geo::P1_BYTES + Geo::P0_BYTES);
-        unsigned char *stg = st_base + j * Geo::STAGE;
-        tma_load3(smem_u32(stg), &D.tm_p1[W], 4 * (G0 - 1), X0 - 3, s_fi[0], b);
-        tma_load3(smem_u32(stg + Geo::P0_OFF), &D.tm_p0[W], 4 * G0, X0, s_fi[1], b);
-    };
     if (tid == 0) {
-        for (int j = 0; j < NST; ++j) mbar_init(smem_u32(&bar[j]), 1);
+        for (int j = 0; j < NST; ++j) {
+            mbar_init(smem_u32(&full[j]), 1);
+            mbar_init(smem_u32(&empty[j]), NW);
+        }
+        mbar_init(smem_u32(&cfbar), 1);
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
-    __syncthreads();  // barriers and the per-shot scalars
-    if (tid == 0) {
-        // the coefficient tiles join the first stage's transaction
-        tmap_acquire(&A.tm_cf[W]);
-        mbar_expect(smem_u32(&bar[0]), Geo::CF_BYTES);
-        tma_load3(smem_u32(smem), &A.tm_cf[W], 4 * G0, X0, 0, smem_u32(&bar[0]));
-        for (int j = 0; j < NST && j < n; ++j) issue(j, j);
+    __syncthreads();  // barriers and the per-shot scalars; no block-wide barrier follows
+    const int X0 = blockIdx.x * TX, G0 = blockIdx.z * TG;
+    unsigned char *st_base = smem + Geo::ST_OFF;
+
+    if (warp == NW) {
+        // ---- producer: coefficients once, then shot j into stage j % NST once every
+        // consumer warp has released that stage's previous shot
+        if (lane != 0) return;
+        mbar_arrive_expect(smem_u32(&cfbar), Geo::CF_BYTES);
+        tma_load3(smem_u32(smem), &tm_cf, 4 * G0, X0, 0, smem_u32(&cfbar));
+        const int i1 = s_fi[0], i0 = s_fi[1];
+        int issued = 0;
+        for (int j = 0; j < n; ++j) {
+            const int st = j % NST;
+            if (j >= NST && !mbar_wait(smem_u32(&empty[st]), (j / NST - 1) & 1)) {
+                atomicExch(err, 1);
+                break;
+            }
+            const int sg = cb + j - shot_base;  // shot index in the pool
+            const unsigned b = smem_u32(&full[st]);
+            mbar_arrive_expect(b, Geo::P1_BYTES + Geo::P0_BYTES);
+            unsigned char *stg = st_base + st * Geo::STAGE;
+            tma_load4(smem_u32(stg), &tm_p1, 4 * (G0 - 1), X0 - 3, i1, sg, b);
+            tma_load4(smem_u32(stg + Geo::P0_OFF), &tm_p0, 4 * G0, X0, i0, sg, b);
+            issued = j + 1;
+        }
+        // keep the block alive until every copy it issued has landed (the consumers wait for
+        // them too, unless they gave up)
+        mbar_wait(smem_u32(&cfbar), 0);
+        for (int j = max(0, issued - NST); j < issued; ++j) mbar_wait(smem_u32(&full[j % NST]), (j / NST) & 1);
+        return;
     }
 
     // ---- per-thread constants
@@ -339,18 +374,8 @@ __global__ void __launch_bounds__(TG *TX) k_tile(const ShotDesc *__restrict__ sh
     const float4(*scf)[TX][TG] = reinterpret_cast<const float4(*)[TX][TG]>(smem);
     float4 cf[6];
 
-    int i = 0;
-    for (; i < n; ++i) {
-        const int st = i % NST;
-        const int ok = __syncthreads_and(tid == 0 ? (int)mbar_wait(smem_u32(&bar[st]), (i / NST) & 1) : 1);
-        if (!ok) break;
-        // every thread is past shot i-1: its stage takes shot i-1+NST
-        if (tid == 0 && i >= 1 && i - 1 + NST < n) issue((i - 1) % NST, i - 1 + NST);
-        if (i == 0) {
-#pragma unroll
-            for (int f = 0; f < 6; ++f) cf[f] = scf[f][k][threadIdx.x];
-        }
-        if (!mine) continue;
+    // one shot of the chunk from ring stage st: stencil, fused epilogue, store
+    auto consume_shot = [&](int i, int st) {
         const unsigned char *stg = st_base + st * Geo::STAGE;
         const float4(*sp1)[TG + 2] = reinterpret_cast<const float4(*)[TG + 2]>(stg);
         const float4(*sp0)[TG] = reinterpret_cast<const float4(*)[TG]>(stg + Geo::P0_OFF);
@@ -424,12 +449,27 @@ __global__ void __launch_bounds__(TG *TX) k_tile(const ShotDesc *__restrict__ sh
                 if (z > pml && z <= 2 * pml) out[colx + 2 * pml - z] = comp(mir, j);
             }
         }
+    };
+
+    {  // coefficient tiles, once for all shots
+        bool ok = mbar_wait(smem_u32(&cfbar), 0);
+        if (!__all_sync(0xffffffffu, ok)) {
+            if (lane == 0) atomicExch(err, 1);
+            return;
+        }
+#pragma unroll
+        for (int f = 0; f < 6; ++f) cf[f] = scf[f][k][threadIdx.x];
     }
-    if (i < n && tid == 0) {
-        // a copy did not land in time: report it and let the copies in flight finish
-        atomicExch(err, 1);
-        const int last = min(n, (i > 0 ? i - 1 : 0) + NST);
-        for (int j = i; j < last; ++j) mbar_wait(smem_u32(&bar[j % NST]), (j / NST) & 1);
+    for (int i = 0; i < n; ++i) {
+        const int st = i % NST;
+        bool ok = mbar_wait(smem_u32(&full[st]), (i / NST) & 1);
+        if (!__all_sync(0xffffffffu, ok)) {  // the warp gives up as one
+            if (lane == 0) atomicExch(err, 1);
+            break;
+        }
+        if (mine) consume_shot(i, st);
+        __syncwarp();
+        if (lane == 0) mbar_arrive(smem_u32(&empty[st]));
     }
 }
 
