@@ -775,18 +775,19 @@ static TileFn tile_fn_nst(int nst)
     return nst == 2 ? tile_fn<TX, 2, MATH>() : nst == 4 ? tile_fn<TX, 4, MATH>() : tile_fn<TX, 3, MATH>();
 }
 
-// shots per block: split the group into equal chunks (at most TILE_CH_MAX shots each) and
-// take the fewest chunks whose grid fills its last wave of resident blocks about as well
-// as the best split does
+// shots per block: split the group into equal chunks (at most 12 shots each, the measured
+// best for 60-shot groups) and take the fewest chunks whose grid fills its last wave of
+// resident blocks about as well as the best split does
 static int pick_chunk(int tiles, int nshot, int resident)
 {
+    const int cap = 12;
     const int slots = 148 * resident;
     auto fill = [&](int nch) {
         const long long blocks = (long long)tiles * nch;
         const long long waves = (blocks + slots - 1) / slots;
         return (double)blocks / (double)(waves * slots);
     };
-    const int nmin = (nshot + TILE_CH_MAX - 1) / TILE_CH_MAX;
+    const int nmin = (nshot + cap - 1) / cap;
     double best = 0.0;
     for (int nch = nmin; nch <= nshot; nch++) best = std::max(best, fill(nch));
     for (int nch = nmin; nch <= nshot; nch++)

@@ -167,6 +167,7 @@ __device__ __forceinline__ void mbar_arrive(unsigned bar)
 {
     asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(bar) : "memory");
 }
+// one try (the hardware may suspend the thread briefly while the phase is open)
 __device__ __forceinline__ bool mbar_try(unsigned bar, unsigned parity)
 {
     unsigned done;
@@ -355,6 +356,8 @@ __global__ void __launch_bounds__(TG *(TX + 2))
     const bool hess = kind == K_FWD1 && A.hessian && (it % MST == 0);
     const bool image = kind == K_ADJ && (it % MST == 0);
     const bool acc_here = mine && (hess || image) && z0 + 3 >= pml && z0 < pml + A.nz && x >= pml && x < pml + A.nxx;
+    const bool fs_tile = A.fs && 4 * G0 <= 2 * pml;  // tile holds free-surface or mirrored rows
+    const bool acc_tile = hess || image;
     const long long colx = (long long)x * A.ld, col = colx + z0;
     const float invdx = A.invdx, invdz = A.invdz, invdtdt = A.invdtdt;
     PkConst K;
@@ -394,8 +397,16 @@ __global__ void __launch_bounds__(TG *(TX + 2))
                 if (z0 + 3 < zlo || z0 + 3 > zhi) v.w = 0.f;
             }
         }
-        const int isz = s_isz[i];
-        const bool src_here = x == s_isx[i] && isz >= z0 && isz < z0 + 4;
+        // most tiles need none of the rare parts of the epilogue: decided per tile and shot
+        const int isx = s_isx[i], isz = s_isz[i];
+        const bool src_tile = (fwd || kind == K_REP) && isx >= X0 && isx < X0 + TX && isz >= 4 * G0 &&
+                              isz < 4 * (G0 + TG);
+        const bool inj_tile = inject && 4 * (G0 + TG) > s_rz0[i] && 4 * G0 <= s_rz1[i];
+        if (!(fs_tile || acc_tile || src_tile || inj_tile)) {
+            *reinterpret_cast<float4 *>(s_out[i] + col) = v;
+            return;
+        }
+        const bool src_here = x == isx && isz >= z0 && isz < z0 + 4;
         // forward: the source enters before the free surface, in double (propagation.c:558-564)
         if (fwd && src_here) setc(v, isz - z0, (float)__dadd_rn((double)comp(v, isz - z0), s_srcd[i]));
         float4 mir = zero4;
