@@ -283,26 +283,55 @@ class DropIn:
 
 
 # ------------------------------------------------------------------ roofline
+TRAFFIC = os.path.join(ROOT, "profiles", "k_tile_forward_60shots_traffic.json")
+
+
 def step_roofline(ctx, E, peaks):
-    """Time the fused step kernel alone: the batched forward pass (one k_step launch per time
-    step, all 60 shots per launch), device time from CUDA events on the engine's stream."""
+    """Time the fused step kernel alone: the batched forward pass (one k_tile launch per time
+    step, all 60 shots per launch), device time from CUDA events on the engine's stream.
+    `traffic` is the DRAM read + write of one such launch from the committed ncu capture of the
+    same launch (60 shots of the 221 x 601 survey, the size this bench runs)."""
     ctx.run(0, path=E.PATH_BATCHED)
     ctx.run(0, path=E.PATH_BATCHED)
     st = ctx.stats()
     per_launch_ms = st["ms"] / st["kernel_launches"]
     cells_per_launch = st["cell_updates"] / NT
     # algorithmic bytes per cell-update with S shots stepping together on one coefficient set:
-    # p1 read + p0 read + p2 write (12 B) + 5 coefficient planes shared by S shots (20 B / S)
+    # p1 read + p0 read + p2 write (12 B) + 6 coefficient planes read once for the S shots (24 B / S)
     S = NSHOT
-    bytes_per_launch = cells_per_launch * (12.0 + 20.0 / S)
+    bpc = 12.0 + 24.0 / S
+    bytes_per_launch = cells_per_launch * bpc
     achieved = bytes_per_launch / (per_launch_ms * 1e-3) / 1e9
     peak = peaks.get("hbm_gbs")
+    traffic = None
+    if os.path.exists(TRAFFIC):
+        t = json.load(open(TRAFFIC))
+        traffic = t["dram_read_bytes"] + t["dram_write_bytes"]
     return {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
-            "frac": achieved / peak if peak else None,
-            "traffic": None, "kernel": "k_step (batched forward, 60 shots per launch)",
+            "frac": achieved / peak if peak else None, "traffic": traffic,
+            "traffic_vs_algorithmic": traffic / bytes_per_launch if traffic else None,
+            "kernel": "k_tile (batched forward, 60 shots per launch)",
             "launch_us": per_launch_ms * 1e3, "gcells_per_s": cells_per_launch / (per_launch_ms * 1e-3) / 1e9,
-            "bytes_per_cell_update": 12.0 + 20.0 / S, "shots_sharing_coefficients": S,
-            "peak_source": "measured" if peak else "fallback"}
+            "bytes_per_cell_update": bpc, "algorithmic_bytes_per_launch": bytes_per_launch,
+            "shots_sharing_coefficients": S, "peak_source": "measured" if peak else "fallback"}
+
+
+def step_case(nshot, nt):
+    """A short batched forward on the survey model (the step kernel's launch shape at full size)
+    for profilers: `ncu ... python bench.py --step-case 60 40`."""
+    from fwiedu import engine as E
+    from fwiedu import models as M
+    vp = M.layered_model(NZ, NX, seed=0)
+    rho = M.gardner(vp)
+    src = M.ricker(nt, DT, 10.0, 0.15)
+    sv = M.line_survey(NZ, NX, DX, DX, DT, nt, nshot, src, spacing_cells=max(1, (NX - 20) // nshot), first_cell=10)
+    ctx = E.Context(0)
+    ctx.set_model(vp, rho, DX, DX, DT, nt, PML, FS)
+    ctx.set_shots(M.survey_shots(sv))
+    ctx.run(0, path=E.PATH_BATCHED)
+    st = ctx.stats()
+    print(f"step case: {nshot} shots, {nt} steps, {st['kernel_launches']} launches, {st['ms']:.2f} ms", flush=True)
+    ctx.close()
 
 
 def main():
@@ -313,8 +342,12 @@ def main():
     ap.add_argument("--impl", default="mine", choices=["mine", "reference"])
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline sample")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--step-case", nargs=2, type=int, metavar=("SHOTS", "NT"),
+                    help="profiling case: one batched forward of SHOTS shots of the survey for NT steps, no JSON line")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
+    if args.step_case:
+        return step_case(*args.step_case)
     if args.impl == "reference":
         return run_reference_arm(args)
 
