@@ -133,6 +133,10 @@ struct fwi_ctx {
     fwi_stats stats{};
     int math = 0;  // 0: bit-exact arithmetic, 1: contracted multiply-adds
     int *d_err = nullptr;  // set by a step kernel whose tile copy did not complete
+    // exchange hook of a shot-sharded run (one context per GPU): sums device doubles over ranks
+    fwi_allreduce_fn ar_fn = nullptr;
+    void *ar_user = nullptr;
+    double *d_xchg = nullptr;  // the scalar sums handed to the hook
     // frame pools: the frame blocks of a shot group, consecutive (key: first shot of the
     // group on the batched path, -1 for the plain path's single shot)
     struct Pool {
@@ -221,8 +225,8 @@ extern "C" int fwi_ctx_destroy(fwi_ctx *c)
     for (float *p : c->d_pre) cudaFree(p);
     for (float *p : c->d_pre_alt) cudaFree(p);
     cudaFree(c->d_vp); cudaFree(c->d_rho); cudaFree(c->d_grad); cudaFree(c->d_prec);
-    cudaFree(c->d_gc); cudaFree(c->d_hc); cudaFree(c->d_red); cudaFree(c->d_scratch); cudaFree(c->d_desc);
-    cudaFree(c->d_err);
+    cudaFree(c->d_gc); cudaFree(c->d_red); cudaFree(c->d_scratch); cudaFree(c->d_desc);
+    cudaFree(c->d_err); cudaFree(c->d_xchg);
     cudaEventDestroy(c->ev0); cudaEventDestroy(c->ev1);
     cudaStreamDestroy(c->stream);
     delete c;
@@ -247,7 +251,7 @@ static int set_model_common(fwi_ctx *c, int nz, int nx, float dx, float dz, floa
         }
         c->plans.clear();
         dfree(c, c->d_vp, 0); dfree(c, c->d_rho, 0);
-        dfree(c, c->d_grad, 0); dfree(c, c->d_prec, 0); dfree(c, c->d_gc, 0); dfree(c, c->d_hc, 0);
+        dfree(c, c->d_grad, 0); dfree(c, c->d_prec, 0); dfree(c, c->d_gc, 0);
         c->d_vp = c->d_rho = c->d_grad = c->d_prec = nullptr;
         c->d_gc = c->d_hc = nullptr;
         size_t m = (size_t)nz * nx;
@@ -255,8 +259,8 @@ static int set_model_common(fwi_ctx *c, int nz, int nx, float dx, float dz, floa
         TRY(dmalloc(c, (void **)&c->d_rho, m * 4));
         TRY(dmalloc(c, (void **)&c->d_grad, m * 4));
         TRY(dmalloc(c, (void **)&c->d_prec, m * 4));
-        TRY(dmalloc(c, (void **)&c->d_gc, m * 8));
-        TRY(dmalloc(c, (void **)&c->d_hc, m * 8));
+        TRY(dmalloc(c, (void **)&c->d_gc, 2 * m * 8));  // FP64 stacks of g and H, one block for the exchange
+        c->d_hc = c->d_gc + m;
     }
     c->nz = nz; c->nx = nx; c->nt = nt; c->pml = pml; c->fs = fs;
     c->dx = dx; c->dz = dz; c->dt = dt;
@@ -1008,6 +1012,39 @@ static int shot_precondition(fwi_ctx *c, const std::vector<ShotRun *> &rs)
     return FWI_OK;
 }
 
+// ---------------------------------------------------------------- exchange between ranks
+// The hook replaces `count` device doubles by their sum over the ranks, ordered on the
+// engine's stream.  Without a hook the context is the whole survey and nothing happens.
+static int exchange(fwi_ctx *c, double *dev, size_t count)
+{
+    if (!c->ar_fn) return FWI_OK;
+    const int rc = c->ar_fn(dev, count, (void *)c->stream, c->ar_user);
+    if (rc != 0) return fail(FWI_ERR_CUDA, "all-reduce hook failed (%d)", rc);
+    CK(cudaGetLastError());
+    return FWI_OK;
+}
+
+// host scalars summed over the ranks through the hook (a round trip through d_xchg)
+static int exchange_scalars(fwi_ctx *c, double *v, int n)
+{
+    if (!c->ar_fn) return FWI_OK;
+    if (n > 8) return fail(FWI_ERR_ARG, "too many scalars for one exchange");
+    if (!c->d_xchg) TRY(dmalloc(c, (void **)&c->d_xchg, 8 * sizeof(double)));
+    CK(cudaMemcpyAsync(c->d_xchg, v, n * sizeof(double), cudaMemcpyHostToDevice, c->stream));
+    TRY(exchange(c, c->d_xchg, (size_t)n));
+    CK(cudaMemcpyAsync(v, c->d_xchg, n * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+    return FWI_OK;
+}
+
+extern "C" int fwi_ctx_set_allreduce(fwi_ctx *c, fwi_allreduce_fn fn, void *user)
+{
+    if (!c) return fail(FWI_ERR_ARG, "ctx is NULL");
+    c->ar_fn = fn;
+    c->ar_user = user;
+    return FWI_OK;
+}
+
 static int stack_and_precondition(fwi_ctx *c, const std::vector<ShotRun *> &rs, int precondition)
 {
     const long long m = (long long)c->nz * c->nx;
@@ -1025,8 +1062,11 @@ static int stack_and_precondition(fwi_ctx *c, const std::vector<ShotRun *> &rs, 
     StackShot *d;
     TRY(put(c, ss, &d, 0));
     k_stack<<<592, 256, 0, c->stream>>>(d, (int)ss.size(), c->nz, c->nx, precondition == 1, c->d_gc, c->d_hc);
+    c->launches++;
+    // the one exchange step of a sharded gradient: both FP64 stacks summed over the ranks
+    TRY(exchange(c, c->d_gc, 2 * (size_t)m));
     k_to_float<<<592, 256, 0, c->stream>>>(c->d_gc, c->d_grad, m);
-    c->launches += 2;
+    c->launches++;
     if (precondition == 1) {
         k_to_float<<<592, 256, 0, c->stream>>>(c->d_hc, c->d_prec, m);
         SumDesc s{};
@@ -1321,6 +1361,7 @@ extern "C" int fwi_ctx_objective(fwi_ctx *c, double *out)
         TRY(reduce(c, part, h));
         for (size_t i = 0; i < part.size(); i++) acc += h[2 * i];
     }
+    TRY(exchange_scalars(c, &acc, 1));
     *out = 0.5 * acc;
     return FWI_OK;
 }
@@ -1565,6 +1606,7 @@ extern "C" int fwi_ctx_fwi_iteration(fwi_ctx *c, const fwi_iter_params *p, fwi_i
     c->launches += 2;
     double f1;
     TRY(sum_gathers(c, c->d_pre, nullptr, 1, &f1, nullptr));
+    TRY(exchange_scalars(c, &f1, 1));
     const float fun1 = (float)(0.5 * f1);
     CK(cudaMemcpyAsync(d_slow, c->slow.data(), m * 4, cudaMemcpyHostToDevice, c->stream));
     SumDesc sd{};
@@ -1605,6 +1647,11 @@ extern "C" int fwi_ctx_fwi_iteration(fwi_ctx *c, const fwi_iter_params *p, fwi_i
     double f2, num, den;
     TRY(sum_gathers(c, c->d_pre, nullptr, 1, &f2, nullptr));
     TRY(sum_gathers(c, c->d_pre_alt, &c->d_pre, 3, &num, &den));
+    {
+        double v[3] = {f2, num, den};
+        TRY(exchange_scalars(c, v, 3));
+        f2 = v[0]; num = v[1]; den = v[2];
+    }
     const float fun2 = (float)(0.5 * f2);
     const float steplen = den == 0.0 ? 0.0f : (float)(num / den);
     // model update (acoustic2d_fwi.c:452-465)

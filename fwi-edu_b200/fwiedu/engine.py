@@ -176,6 +176,10 @@ def propagation(vp, rho, shots, dx, dz, dt, nt, pml, fs, freq, filt, preconditio
     return pre, grad
 
 
+# fwi_allreduce_fn: int (*)(double *dev, size_t count, void *stream, void *user)
+ALLREDUCE_FN = C.CFUNCTYPE(C.c_int, C.c_void_p, C.c_size_t, C.c_void_p, C.c_void_p)
+
+
 class Context:
     """Device-resident engine context (fwi_ctx_*)."""
 
@@ -257,6 +261,29 @@ class Context:
         rho = np.empty_like(vp)
         _check(self.L.fwi_ctx_get_model(self.h, _ptr(vp), _ptr(rho)))
         return vp, rho
+
+    def set_allreduce(self, fn):
+        """Install the exchange hook of a shot-sharded run (fwi_ctx_set_allreduce).
+
+        ``fn(dev_ptr, count, stream_ptr)`` must replace ``count`` FP64 values at device address
+        ``dev_ptr`` by their sum over all ranks, ordered on the engine's CUDA stream
+        ``stream_ptr`` (see fwiedu.dist.device_hook).  ``None`` removes the hook."""
+        if fn is None:
+            self._ar = None
+            _check(self.L.fwi_ctx_set_allreduce(self.h, None, None))
+            return
+
+        def _cb(dev, count, stream, user):
+            try:
+                fn(int(dev or 0), int(count), int(stream or 0))
+                return 0
+            except Exception:  # reported to the engine as a failed exchange
+                import traceback
+                traceback.print_exc()
+                return 1
+
+        self._ar = ALLREDUCE_FN(_cb)  # keep the thunk alive as long as the context
+        _check(self.L.fwi_ctx_set_allreduce(self.h, self._ar, None))
 
     def stats(self):
         s = FwiStats()

@@ -179,6 +179,19 @@ typedef struct {
 } fwi_stats;
 FWI_API int fwi_ctx_stats(fwi_ctx *ctx, fwi_stats *out);
 
+/* Shot-sharded runs (one context per GPU, each holding a share of the survey's shots and the
+ * whole model).  The path has one exchange step per gradient: the FP64 stacks of the gradient
+ * and of the pseudo-Hessian (propagation.c:953-976 stacks them over shots) and the
+ * scalar sums of the FWI loop (misfit, step-length numerator and denominator,
+ * optimization.c:13-76).  With a hook installed, the engine calls it at each exchange point
+ * with `count` device doubles that the hook must replace, in place, by their sum over all
+ * ranks, enqueued on (or synchronised with) `stream`, the engine's CUDA stream; it returns 0 on
+ * success.  Every rank reaches the same exchange points in the same order.  The global
+ * preconditioning and everything after it then run redundantly on each rank, as in the
+ * reference after its stack.  No counterpart in the reference (it runs on one host). */
+typedef int (*fwi_allreduce_fn)(double *dev, size_t count, void *stream, void *user);
+FWI_API int fwi_ctx_set_allreduce(fwi_ctx *ctx, fwi_allreduce_fn fn, void *user);
+
 /* one iteration of the FWI loop of acoustic2d_fwi.c:411-465 on the context's model, shots and
  * observed data, everything between the two propagations on the device:
  * gradient (problem 1) -> cos^2 smoothing along z (rz) then x (rx) -> fun1 = misfit ->

@@ -117,6 +117,31 @@ class Port:
             raise ValueError(f"orc_forward: status {rc}")
         return tr
 
+    def shot_gradient(self, shot, vp, rho, dx, dz, dt, nt, pml, fs, freq, filt, precondition, obs):
+        """One shot's gradient and preconditioner on its window (orc_shot_gradient, FP32 port):
+        (adjoint source, g, h), g and h of shape (ix_max - ix_min + 1, nz)."""
+        if self.precision != 32:
+            raise ValueError("shot_gradient wraps the FP32 port")
+        vp, rho = _f32(vp), _f32(rho)
+        nx, nz = vp.shape
+        nxx = shot.ix_max - shot.ix_min + 1
+        pre = np.zeros((len(shot.igx), shot.ns), np.float32)
+        g = np.zeros((nxx, nz), np.float32)
+        h = np.zeros((nxx, nz), np.float32)
+        rc = self.lib.orc_shot_gradient(C.byref(self._shot(shot)), _ptr(vp), _ptr(rho), nz, nx, C.c_float(dx),
+                                        C.c_float(dz), C.c_float(dt), nt, pml, fs, C.c_float(freq), int(filt),
+                                        precondition, _ptr(_f32(obs)), _ptr(pre), _ptr(g), _ptr(h))
+        self._keep.clear()
+        if rc:
+            raise ValueError(f"orc_shot_gradient: status {rc}")
+        return pre, g, h
+
+    def global_precondition(self, grad, precond, alpha=0.005):
+        """orc_global_precondition on float32 arrays, in place."""
+        n = grad.size
+        self.lib.orc_global_precondition(_ptr(grad), _ptr(precond), n, C.c_float(alpha))
+        return grad
+
     def propagation(self, vp, rho, shots, dx, dz, dt, nt, pml, fs, freq, filt, precondition, problem,
                     obs=None, pre=None):
         """Mirror of iso_acoustic2d_propagation; returns (pre traces list, grad or None)."""
