@@ -247,6 +247,7 @@ __global__ void __launch_bounds__(TG *(TX + 2))
     __shared__ double s_srcd[TILE_CH_MAX];
     __shared__ float s_srcf[TILE_CH_MAX];
     __shared__ int s_isx[TILE_CH_MAX], s_isz[TILE_CH_MAX], s_rz0[TILE_CH_MAX], s_rz1[TILE_CH_MAX];
+    __shared__ bool s_spec[TILE_CH_MAX];
     __shared__ int s_fi[2];  // frames of p1 and p0 (the same for every shot of the chunk)
 
     const int4 pw = prog[L];
@@ -296,6 +297,13 @@ __global__ void __launch_bounds__(TG *(TX + 2))
         s_srcf[tid] = kind == K_REP ? D.srcf[it] : 0.0f;
         s_rz0[tid] = D.rz0;
         s_rz1[tid] = D.rz1;
+        // does this tile need the rare parts of the epilogue for this shot (its source, its
+        // receiver rows for the adjoint injection)?
+        const int X0t = blockIdx.x * TX, Z0t = 4 * blockIdx.z * TG;
+        const bool src_t = (fwd || kind == K_REP) && D.isx >= X0t && D.isx < X0t + TX && D.isz >= Z0t &&
+                           D.isz < Z0t + 4 * TG;
+        const bool inj_t = kind == K_ADJ && it >= 1 && Z0t + 4 * TG > D.rz0 && Z0t <= D.rz1;
+        s_spec[tid] = src_t || inj_t;
         if (tid == 0) {
             s_fi[0] = i1;
             s_fi[1] = i0;
@@ -350,13 +358,19 @@ __global__ void __launch_bounds__(TG *(TX + 2))
     const bool zfd = z0 + 3 >= zlo && z0 <= zhi;
     const bool zpart = z0 < zlo || z0 + 3 > zhi;  // group straddles the edge of the updated rows
     const bool any = mine && zfd && x >= 3 && x <= Nx - 4;
-    const bool fs_top = A.fs && mine && z0 <= 2 * pml;  // the free-surface row or the rows it mirrors
+    // Free surface.  The reference sets row pml to -0 and mirrors rows pml+1..2pml into rows
+    // pml-1..0 (propagation.c:76-101).  Only the three mirrored rows next to the surface are ever
+    // read again (the stencil updates rows >= pml and reaches three rows up; receivers, imaging
+    // and the Hessian lie at rows >= pml), so only rows pml+1..pml+3 are mirrored here: every
+    // seismogram and gradient is the reference's, and the rows above pml-3 are never written.
+    const int fs_hi = min(2 * pml, pml + 3);  // last mirrored source row
+    const bool fs_top = A.fs && mine && z0 <= fs_hi;  // the surface row, the mirror source rows, or above
     const int jpml = (pml >= z0 && pml < z0 + 4) ? pml - z0 : -1;
     const bool inject = kind == K_ADJ && it >= 1;
     const bool hess = kind == K_FWD1 && A.hessian && (it % MST == 0);
     const bool image = kind == K_ADJ && (it % MST == 0);
     const bool acc_here = mine && (hess || image) && z0 + 3 >= pml && z0 < pml + A.nz && x >= pml && x < pml + A.nxx;
-    const bool fs_tile = A.fs && 4 * G0 <= 2 * pml;  // tile holds free-surface or mirrored rows
+    const bool fs_tile = A.fs && 4 * G0 <= fs_hi;  // tile holds the surface, mirror or rows above
     const bool acc_tile = hess || image;
     const long long colx = (long long)x * A.ld, col = colx + z0;
     const float invdx = A.invdx, invdz = A.invdz, invdtdt = A.invdtdt;
@@ -398,14 +412,11 @@ __global__ void __launch_bounds__(TG *(TX + 2))
             }
         }
         // most tiles need none of the rare parts of the epilogue: decided per tile and shot
-        const int isx = s_isx[i], isz = s_isz[i];
-        const bool src_tile = (fwd || kind == K_REP) && isx >= X0 && isx < X0 + TX && isz >= 4 * G0 &&
-                              isz < 4 * (G0 + TG);
-        const bool inj_tile = inject && 4 * (G0 + TG) > s_rz0[i] && 4 * G0 <= s_rz1[i];
-        if (!(fs_tile || acc_tile || src_tile || inj_tile)) {
+        if (!(fs_tile || acc_tile || s_spec[i])) {
             *reinterpret_cast<float4 *>(s_out[i] + col) = v;
             return;
         }
+        const int isx = s_isx[i], isz = s_isz[i];
         const bool src_here = x == isx && isz >= z0 && isz < z0 + 4;
         // forward: the source enters before the free surface, in double (propagation.c:558-564)
         if (fwd && src_here) setc(v, isz - z0, (float)__dadd_rn((double)comp(v, isz - z0), s_srcd[i]));
@@ -457,7 +468,7 @@ __global__ void __launch_bounds__(TG *(TX + 2))
 #pragma unroll
             for (int j = 0; j < 4; ++j) {
                 const int z = z0 + j;
-                if (z > pml && z <= 2 * pml) out[colx + 2 * pml - z] = comp(mir, j);
+                if (z > pml && z <= fs_hi) out[colx + 2 * pml - z] = comp(mir, j);
             }
         }
     };
