@@ -66,6 +66,34 @@ static __global__ void k_gather(const GatherDesc *__restrict__ gd, int mode)
     }
 }
 
+// taper_traces (common.c:796-895) in place on one [ntr][ns] gather per blockIdx.y: the time
+// factor first, then the trace factor, as k_gather applies them
+struct TaperDesc {
+    float *a;
+    const float *tct, *tcr;
+    int ns, ntr, Lt, Lr;
+};
+static __global__ void k_taper(const TaperDesc *__restrict__ td)
+{
+    const TaperDesc &D = td[blockIdx.y];
+    const long long n = (long long)D.ns * D.ntr;
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+        const int r = (int)(i / D.ns), k = (int)(i % D.ns);
+        float v = D.a[i];
+        if (D.Lt > 0) {
+            if (k <= D.Lt) v = __fmul_rn(v, D.tct[D.Lt - k]);
+            const int kb = D.ns - D.Lt - 1;
+            if (k >= kb) v = __fmul_rn(v, D.tct[k - kb]);
+        }
+        if (D.Lr > 0) {
+            if (r <= D.Lr) v = __fmul_rn(v, D.tcr[D.Lr - r]);
+            const int rb = D.ntr - D.Lr - 1;
+            if (r >= rb) v = __fmul_rn(v, D.tcr[r - rb]);
+        }
+        D.a[i] = v;
+    }
+}
+
 struct FinDesc {
     const double *acc;    // [Nx][ld] accumulator
     float *out;           // [nxx][nz] window, FP32 as the reference keeps per-shot fields

@@ -14,6 +14,7 @@
 // group go into every launch and the whole launch sequence is captured once as
 // a CUDA graph and replayed; on the plain path shots run one after another, one
 // launch per step, as the reference's shot loop does (propagation.c:857, :895).
+#include <cublas_v2.h>
 #include <cuda.h>
 #include <cudaTypedefs.h>  // PFN_cuTensorMapEncodeTiled
 #include <cuda_runtime.h>
@@ -24,6 +25,7 @@
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
+#include <cstdint>
 #include <deque>
 #include <map>
 #include <memory>
@@ -90,6 +92,7 @@ struct ShotRun {
     ShotDesc d{};
     // per-run host-side extras
     int Lt = 0, Lr = 0;
+    float fpass = 0.f, kpass = 0.f;  // residual filter pass frequency (Hz) and wavenumber (1/m)
     float *d_tct = nullptr, *d_tcr = nullptr;
     float *d_gshot = nullptr, *d_hshot = nullptr;  // [nxx][nz] FP32 per-shot gradient / preconditioner
     bool has_ck = false;
@@ -146,6 +149,11 @@ struct fwi_ctx {
         long long frame = 0;
     };
     std::map<int, Pool> pools;
+    // residual filters and trace interpolation: cuBLAS (pedantic FP32) and the operator matrices
+    cublasHandle_t blas = nullptr;
+    std::map<std::string, std::pair<float *, size_t>> ops;
+    float *d_fft_tmp = nullptr;
+    size_t fft_tmp_bytes = 0;
     long long launches = 0;
     double last_obj = 0.0;
 };
@@ -226,7 +234,9 @@ extern "C" int fwi_ctx_destroy(fwi_ctx *c)
     for (float *p : c->d_pre_alt) cudaFree(p);
     cudaFree(c->d_vp); cudaFree(c->d_rho); cudaFree(c->d_grad); cudaFree(c->d_prec);
     cudaFree(c->d_gc); cudaFree(c->d_red); cudaFree(c->d_scratch); cudaFree(c->d_desc);
-    cudaFree(c->d_err); cudaFree(c->d_xchg);
+    cudaFree(c->d_err); cudaFree(c->d_xchg); cudaFree(c->d_fft_tmp);
+    for (auto &kv : c->ops) cudaFree(kv.second.first);
+    if (c->blas) cublasDestroy(c->blas);
     cudaEventDestroy(c->ev0); cudaEventDestroy(c->ev1);
     cudaStreamDestroy(c->stream);
     delete c;
@@ -629,6 +639,8 @@ static int prepare_taper(fwi_ctx *c, ShotRun *r, float freq)
     if (Lr < 0) Lr = 0;
     r->Lt = Lt;
     r->Lr = Lr;
+    r->fpass = freq;
+    r->kpass = kpass;
     std::vector<float> a(Lt + 1), b(Lr + 1);
     if (Lt > 0) fwi_taper_coefs(Lt, a.data());
     if (Lr > 0) fwi_taper_coefs(Lr, b.data());
@@ -923,7 +935,7 @@ static int reduce(fwi_ctx *c, std::vector<SumDesc> sd, std::vector<double> &out_
 }
 
 // ---------------------------------------------------------------- runs
-static int gather(fwi_ctx *c, const std::vector<ShotRun *> &rs, int mode, bool with_adj)
+static int gather(fwi_ctx *c, const std::vector<ShotRun *> &rs, int mode, bool with_adj, bool trace_taper = true)
 {
     std::vector<GatherDesc> gd;
     int maxns = 1, maxtr = 1;
@@ -938,7 +950,7 @@ static int gather(fwi_ctx *c, const std::vector<ShotRun *> &rs, int mode, bool w
         g.ns = r->d.ns;
         g.ntr = r->d.ntr;
         g.Lt = mode == 1 ? r->Lt : 0;
-        g.Lr = mode == 1 ? r->Lr : 0;
+        g.Lr = mode == 1 && trace_taper ? r->Lr : 0;
         g.adj_rows = c->nt;
         gd.push_back(g);
         maxns = std::max(maxns, g.ns);
@@ -950,6 +962,130 @@ static int gather(fwi_ctx *c, const std::vector<ShotRun *> &rs, int mode, bool w
     k_gather<<<grid, dim3(32, 8), 0, c->stream>>>(d, mode);
     c->launches++;
     CK(cudaGetLastError());
+    return FWI_OK;
+}
+
+static __global__ void k_to_time_major(const float *__restrict__ a, float *__restrict__ out, int ntr, int ns, int nt);
+
+// ---------------------------------------------------------------- residual filters
+static int blas_ok(cublasStatus_t st, const char *what)
+{
+    if (st != CUBLAS_STATUS_SUCCESS) return fail(FWI_ERR_CUDA, "%s failed (cuBLAS status %d)", what, (int)st);
+    return FWI_OK;
+}
+
+static int get_blas(fwi_ctx *c, cublasHandle_t *out)
+{
+    if (!c->blas) {
+        TRY(blas_ok(cublasCreate(&c->blas), "cublasCreate"));
+        // plain FP32 products and sums: no TF32 or other reduced-precision modes
+        TRY(blas_ok(cublasSetMathMode(c->blas, CUBLAS_PEDANTIC_MATH), "cublasSetMathMode"));
+    }
+    TRY(blas_ok(cublasSetStream(c->blas, c->stream), "cublasSetStream"));
+    *out = c->blas;
+    return FWI_OK;
+}
+
+static std::string bits(float v)
+{
+    uint32_t u;
+    memcpy(&u, &v, 4);
+    return std::to_string(u);
+}
+
+// an operator matrix built once on the host (FP64 sums, stored as float) and kept on the device
+template <class Build>
+static int device_operator(fwi_ctx *c, const std::string &key, size_t count, Build build, const float **out)
+{
+    auto it = c->ops.find(key);
+    if (it == c->ops.end()) {
+        std::vector<float> h(count);
+        build(h.data());
+        float *d = nullptr;
+        TRY(dmalloc(c, (void **)&d, count * 4));
+        CK(cudaMemcpy(d, h.data(), count * 4, cudaMemcpyHostToDevice));
+        it = c->ops.emplace(key, std::make_pair(d, count * 4)).first;
+    }
+    *out = it->second.first;
+    return FWI_OK;
+}
+
+static int filter_operator(fwi_ctx *c, int filter, int n, float fpass, float fcut, float dt, const float **out)
+{
+    const std::string key = "filter" + std::to_string(filter) + "/" + std::to_string(n) + "/" + bits(fpass) + "/" +
+                            bits(fcut) + "/" + bits(dt);
+    return device_operator(c, key, (size_t)n * n,
+                           [&](float *h) { fwi_filter_operator(filter, n, fpass, fcut, dt, h); }, out);
+}
+
+static int interp_operator(fwi_ctx *c, int ns, int r, int nt, const float **out)
+{
+    const std::string key = "interp/" + std::to_string(ns) + "/" + std::to_string(r) + "/" + std::to_string(nt);
+    return device_operator(c, key, (size_t)nt * ns, [&](float *h) { fwi_interp_operator(ns, r, nt, h); }, out);
+}
+
+static int taper(fwi_ctx *c, float *a, const ShotRun *r, int Lt, int Lr)
+{
+    TaperDesc t{a, r->d_tct, r->d_tcr, r->d.ns, r->d.ntr, Lt, Lr};
+    TaperDesc *d;
+    TRY(put(c, std::vector<TaperDesc>{t}, &d, 0));
+    k_taper<<<dim3(148, 1), 256, 0, c->stream>>>(d);
+    c->launches++;
+    CK(cudaGetLastError());
+    return FWI_OK;
+}
+
+// compute_adjoint_source2d for filters 0/1 (optimization.c:368-415) and the injection layout for
+// sampleRate > 1 (interpolate_traces, common.c:482-582): residual and time taper in k_gather, then
+// per shot the time filter (GEMM with the ns x ns circulant), the trace taper, the trace filter
+// (GEMM with the shot's ntr x ntr circulant), both tapers; the adjoint source for the injection is
+// the interpolation GEMM into adj_t [nt][ntr] (or a transpose for sampleRate 1).
+static int adjoint_source_filtered(fwi_ctx *c, const std::vector<ShotRun *> &rs, int filter, bool with_adj)
+{
+    const bool fft = filter == 0 || filter == 1;
+    TRY(gather(c, rs, 1, false, /*trace_taper=*/!fft));
+    cublasHandle_t h;
+    TRY(get_blas(c, &h));
+    const float one = 1.0f, zero = 0.0f;
+    for (ShotRun *r : rs) {
+        const int ns = r->d.ns, ntr = r->d.ntr;
+        const fwi_shot &s = c->shots[r->shot].s;
+        float *pre = c->d_pre[r->shot];
+        if (fft) {
+            const size_t need = (size_t)ns * ntr * 4;
+            if (need > c->fft_tmp_bytes) {
+                dfree(c, c->d_fft_tmp, c->fft_tmp_bytes);
+                c->d_fft_tmp = nullptr;
+                c->fft_tmp_bytes = 0;
+                TRY(dmalloc(c, (void **)&c->d_fft_tmp, need));
+                c->fft_tmp_bytes = need;
+            }
+            const float *Ct, *Cx;
+            TRY(filter_operator(c, filter, ns, r->fpass, 2.0f * r->fpass, s.dt, &Ct));
+            TRY(filter_operator(c, filter, ntr, r->kpass, 2.0f * r->kpass, s.dtr, &Cx));
+            // time filter: every trace (a column of the [ntr][ns] gather seen column-major) times Ct
+            TRY(blas_ok(cublasSgemm(h, CUBLAS_OP_N, CUBLAS_OP_N, ns, ntr, ns, &one, Ct, ns, pre, ns, &zero,
+                                    c->d_fft_tmp, ns), "time filter GEMM"));
+            TRY(taper(c, c->d_fft_tmp, r, 0, r->Lr));
+            // trace filter: each time sample's vector over the traces times Cx (Cx is symmetric)
+            TRY(blas_ok(cublasSgemm(h, CUBLAS_OP_N, CUBLAS_OP_T, ns, ntr, ntr, &one, c->d_fft_tmp, ns, Cx, ntr, &zero,
+                                    pre, ns), "trace filter GEMM"));
+            TRY(taper(c, pre, r, r->Lt, r->Lr));
+        }
+        if (!with_adj) continue;
+        float *adj = (float *)r->d.adj_t;
+        if (r->d.sr > 1) {
+            const float *M;
+            TRY(interp_operator(c, ns, r->d.sr, c->nt, &M));
+            // adj_t[k][r] = sum_j M[k][j] pre[r][j]: the [nt][ntr] injection layout directly
+            TRY(blas_ok(cublasSgemm(h, CUBLAS_OP_T, CUBLAS_OP_T, ntr, c->nt, ns, &one, pre, ns, M, c->nt, &zero, adj,
+                                    ntr), "interpolation GEMM"));
+        } else {
+            k_to_time_major<<<296, 256, 0, c->stream>>>(pre, adj, ntr, ns, c->nt);
+            c->launches++;
+            CK(cudaGetLastError());
+        }
+    }
     return FWI_OK;
 }
 
@@ -1164,10 +1300,11 @@ static int run_forward_group(fwi_ctx *c, std::vector<ShotRun *> &rs, int problem
     for (ShotRun *r : rs) TRY(zero_initial(c, r, false));
     TRY(run_program(c, "fwd0/" + gkey, prog, shot_base, (int)rs.size(), rs[0], batched));
     if (problem == 2) {
-        if (filter == 0 || filter == 1) return fail(FWI_ERR_UNSUPPORTED, "residual filter %d (FFT) is not built", filter);
+        if (filter < 0 || filter > 2) return fail(FWI_ERR_ARG, "residual filter %d (0 lowpass, 1 bandpass, 2 none)", filter);
         for (ShotRun *r : rs) TRY(prepare_taper(c, r, freq));
     }
-    TRY(gather(c, rs, problem == 2 ? 1 : 0, false));
+    if (problem == 2 && (filter == 0 || filter == 1)) TRY(adjoint_source_filtered(c, rs, filter, false));
+    else TRY(gather(c, rs, problem == 2 ? 1 : 0, false));
     return FWI_OK;
 }
 
@@ -1198,12 +1335,13 @@ static int grad_adjoint(fwi_ctx *c, std::vector<ShotRun *> &rs, bool batched, co
 static int run_gradient_group(fwi_ctx *c, std::vector<ShotRun *> &rs, float freq, int filter, int precondition,
                               bool batched, const std::string &gkey, int shot_base)
 {
-    if (filter == 0 || filter == 1) return fail(FWI_ERR_UNSUPPORTED, "residual filter %d (FFT) is not built", filter);
-    for (ShotRun *r : rs)
-        if (r->d.sr > 1) return fail(FWI_ERR_UNSUPPORTED, "sampleRate > 1 needs FFT trace interpolation (not built)");
+    if (filter < 0 || filter > 2) return fail(FWI_ERR_ARG, "residual filter %d (0 lowpass, 1 bandpass, 2 none)", filter);
     TRY(grad_forward(c, rs, precondition, batched, gkey, shot_base));
     for (ShotRun *r : rs) TRY(prepare_taper(c, r, freq));
-    TRY(gather(c, rs, 1, true));
+    bool interp = false;
+    for (ShotRun *r : rs) interp = interp || r->d.sr > 1;
+    if (filter == 2 && !interp) TRY(gather(c, rs, 1, true));  // residual + tapers straight into adj_t
+    else TRY(adjoint_source_filtered(c, rs, filter, true));
     TRY(grad_adjoint(c, rs, batched, gkey, shot_base));
     if (precondition == 1) TRY(shot_precondition(c, rs));
     return FWI_OK;

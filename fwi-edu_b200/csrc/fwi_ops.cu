@@ -3,13 +3,16 @@
 // front-end written against FWI-EDU links unchanged; each call stages its arrays
 // through one process-wide device workspace.  The device-resident FWI iteration of
 // fwi_engine.cu runs the same kernels without the host round trips.
+#include <cublas_v2.h>
 #include <cuda_runtime.h>
 
 #include <cmath>
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
+#include <map>
 #include <mutex>
+#include <string>
 #include <vector>
 
 #include "../../include/fwi_b200.h"
@@ -64,6 +67,86 @@ bool ops_ready(size_t bytes)
 }
 
 size_t al(size_t b) { return (b + 255) & ~size_t(255); }
+
+// ---- residual filters and interpolation: operator matrices on the device, applied by FP32 GEMM
+cublasHandle_t g_blas = nullptr;
+std::map<std::string, float *> g_opmats;  // built once per (kind, size, parameters) and kept
+
+bool blas_ready()
+{
+    if (!g_blas) {
+        if (cublasCreate(&g_blas) != CUBLAS_STATUS_SUCCESS) {
+            fprintf(stderr, "<error>: cublasCreate failed\n");
+            return false;
+        }
+        cublasSetMathMode(g_blas, CUBLAS_PEDANTIC_MATH);  // plain FP32, no TF32
+    }
+    return cublasSetStream(g_blas, g_ops.st) == CUBLAS_STATUS_SUCCESS;
+}
+
+std::string fbits(float v)
+{
+    unsigned u;
+    memcpy(&u, &v, 4);
+    return std::to_string(u);
+}
+
+const float *op_matrix(const std::string &key, size_t count, void (*build)(float *, const int *, const float *),
+                       const int *ip, const float *fp)
+{
+    auto it = g_opmats.find(key);
+    if (it != g_opmats.end()) return it->second;
+    std::vector<float> h(count);
+    build(h.data(), ip, fp);
+    float *d = nullptr;
+    if (!report(cudaMalloc(&d, count * 4), "cudaMalloc")) return nullptr;
+    if (!report(cudaMemcpy(d, h.data(), count * 4, cudaMemcpyHostToDevice), "copy")) return nullptr;
+    g_opmats[key] = d;
+    return d;
+}
+
+void build_filter(float *h, const int *ip, const float *fp) { fwi_filter_operator(ip[0], ip[1], fp[0], fp[1], fp[2], h); }
+void build_interp(float *h, const int *ip, const float *) { fwi_interp_operator(ip[0], ip[1], ip[2], h); }
+
+// the n x n filter operator of apply_traces_lowpass (0) / apply_traces_bandpass (1)
+const float *filter_matrix(int filter, int n, float fpass, float fcut, float dt)
+{
+    const int ip[2] = {filter, n};
+    const float fp[3] = {fpass, fcut, dt};
+    return op_matrix("f" + std::to_string(filter) + "/" + std::to_string(n) + "/" + fbits(fpass) + "/" + fbits(fcut) +
+                         "/" + fbits(dt),
+                     (size_t)n * n, build_filter, ip, fp);
+}
+
+// y (ntr vectors of n samples, contiguous) = filter applied to x, both on the device
+bool filter_vectors(const float *x, float *y, int n, int nvec, int filter, float fpass, float fcut, float dt)
+{
+    if (!blas_ready()) return false;
+    const float *C = filter_matrix(filter, n, fpass, fcut, dt);
+    if (!C) return false;
+    const float one = 1.0f, zero = 0.0f;
+    return cublasSgemm(g_blas, CUBLAS_OP_N, CUBLAS_OP_N, n, nvec, n, &one, C, n, x, n, &zero, y, n) ==
+           CUBLAS_STATUS_SUCCESS;
+}
+
+// the taper of taper_traces (common.c:796-895) on a [ntr][ns] device gather
+bool taper_device(float *a, int ns, int ntr, int Lt, int Lr, const float *tct, const float *tcr, TaperDesc *d)
+{
+    TaperDesc t{a, tct, tcr, ns, ntr, Lt, Lr};
+    if (!report(cudaMemcpyAsync(d, &t, sizeof(t), cudaMemcpyHostToDevice, g_ops.st), "copy")) return false;
+    k_taper<<<dim3(148, 1), 256, 0, g_ops.st>>>(d);
+    return report(cudaGetLastError(), "k_taper");
+}
+
+// [a][b] -> [b][a] on the device
+__global__ void k_transpose(const float *__restrict__ in, float *__restrict__ out, int a, int b)
+{
+    const long long n = (long long)a * b;
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+        const int ib = (int)(i / a), ia = (int)(i % a);
+        out[i] = in[(long long)ia * b + ib];
+    }
+}
 
 // FP64 sums of one or two operand arrays already on the device
 bool dsum(const float *a, const float *b, long long n, int op, double out[2])
@@ -177,13 +260,15 @@ extern "C" void smooth2D(float **in, float **out, int nx, int nz, int N, int isz
     report(cudaStreamSynchronize(g_ops.st), "smooth2D");
 }
 
-// compute_adjoint_source2d, optimization.c:300-419 (filter 2: residual and tapers)
+// compute_adjoint_source2d, optimization.c:300-419: residual; for filters 0/1 the time taper, time
+// filter, trace taper and trace filter (GEMMs with the circulant operators); both tapers
 extern "C" void compute_adjoint_source2d(Record2D *pre, Record2D *obs, float **vp, float freq, int filter,
                                          Record2D *adj)
 {
     std::lock_guard<std::mutex> lk(g_ops_mu);
-    if (filter == 0 || filter == 1) {
-        fprintf(stderr, "<error>: compute_adjoint_source2d: residual filter %d (FFT) is not built\n", filter);
+    if (filter < 0 || filter > 2) {
+        fprintf(stderr, "<error>: compute_adjoint_source2d: residual filter %d (0 lowpass, 1 bandpass, 2 none)\n",
+                filter);
         return;
     }
     const int ns = adj->ns, ntr = adj->ntr;
@@ -202,16 +287,105 @@ extern "C" void compute_adjoint_source2d(Record2D *pre, Record2D *obs, float **v
     if (Lt > 0) fwi_taper_coefs(Lt, tct.data());
     if (Lr > 0) fwi_taper_coefs(Lr, tcr.data());
     size_t m = (size_t)ns * ntr, nb = al(m * 4);
-    if (!ops_ready(3 * nb + al((Lt + 1) * 4) + al((Lr + 1) * 4))) return;
+    const size_t tb = al((Lt + 1) * 4) + al((Lr + 1) * 4);
+    if (!ops_ready(3 * nb + tb + al(sizeof(TaperDesc)) + 256)) return;
     float *dp = (float *)g_ops.buf, *dob = (float *)(g_ops.buf + nb), *da = (float *)(g_ops.buf + 2 * nb);
     float *dt_ = (float *)(g_ops.buf + 3 * nb), *dr = (float *)(g_ops.buf + 3 * nb + al((Lt + 1) * 4));
+    TaperDesc *td = (TaperDesc *)(g_ops.buf + 3 * nb + tb);
     cudaMemcpyAsync(dp, pre->traces_p[0], m * 4, cudaMemcpyHostToDevice, g_ops.st);
     cudaMemcpyAsync(dob, obs->traces_p[0], m * 4, cudaMemcpyHostToDevice, g_ops.st);
     cudaMemcpyAsync(dt_, tct.data(), (Lt + 1) * 4, cudaMemcpyHostToDevice, g_ops.st);
     cudaMemcpyAsync(dr, tcr.data(), (Lr + 1) * 4, cudaMemcpyHostToDevice, g_ops.st);
-    k_residual_taper<<<296, 256, 0, g_ops.st>>>(dp, dob, da, ns, ntr, Lt, Lr, dt_, dr);
+    if (filter == 2) {
+        k_residual_taper<<<296, 256, 0, g_ops.st>>>(dp, dob, da, ns, ntr, Lt, Lr, dt_, dr);
+    } else {
+        k_residual_taper<<<296, 256, 0, g_ops.st>>>(dp, dob, da, ns, ntr, Lt, 0, dt_, dr);
+        // time filter of every trace, trace taper, filter along the traces of every sample, tapers
+        if (!filter_vectors(da, dp, ns, ntr, filter, freq, 2.0f * freq, adj->dt)) {
+            fprintf(stderr, "<error>: compute_adjoint_source2d: time filter failed\n");
+            return;
+        }
+        if (!taper_device(dp, ns, ntr, 0, Lr, dt_, dr, td)) return;
+        k_transpose<<<296, 256, 0, g_ops.st>>>(dp, dob, ntr, ns);  // [ntr][ns] -> [ns][ntr]
+        if (!filter_vectors(dob, da, ntr, ns, filter, kpass, 2.0f * kpass, adj->dtr)) {
+            fprintf(stderr, "<error>: compute_adjoint_source2d: trace filter failed\n");
+            return;
+        }
+        k_transpose<<<296, 256, 0, g_ops.st>>>(da, dp, ns, ntr);  // back to [ntr][ns]
+        cudaStreamSynchronize(g_ops.st);  // the taper descriptor is reused
+        if (!taper_device(dp, ns, ntr, Lt, Lr, dt_, dr, td)) return;
+        da = dp;
+    }
     cudaMemcpyAsync(adj->traces_p[0], da, m * 4, cudaMemcpyDeviceToHost, g_ops.st);
     report(cudaStreamSynchronize(g_ops.st), "compute_adjoint_source2d");
+}
+
+// apply_traces_lowpass / apply_traces_bandpass (common.c:584-794): ntr traces of nt samples,
+// tr and trs in the alloc2float(nt, ntr) layout (one contiguous block); tr == trs is allowed
+static void traces_filter(float **tr, float **trs, int nt, int ntr, float fpass, float fcut, float dt, int filter,
+                          const char *name)
+{
+    std::lock_guard<std::mutex> lk(g_ops_mu);
+    if (!tr || !trs || nt <= 0 || ntr <= 0) {
+        fprintf(stderr, "<error>: %s: invalid input (nt=%d, ntr=%d)\n", name, nt, ntr);
+        return;
+    }
+    if (fcut <= fpass) {
+        fprintf(stderr, "<error>: %s: fcut must be greater than fpass!\n", name);
+        return;
+    }
+    const size_t m = (size_t)nt * ntr, nb = al(m * 4);
+    if (!ops_ready(2 * nb)) return;
+    float *x = (float *)g_ops.buf, *y = (float *)(g_ops.buf + nb);
+    cudaMemcpyAsync(x, tr[0], m * 4, cudaMemcpyHostToDevice, g_ops.st);
+    if (!filter_vectors(x, y, nt, ntr, filter, fpass, fcut, dt)) {
+        fprintf(stderr, "<error>: %s: filter GEMM failed\n", name);
+        return;
+    }
+    cudaMemcpyAsync(trs[0], y, m * 4, cudaMemcpyDeviceToHost, g_ops.st);
+    report(cudaStreamSynchronize(g_ops.st), name);
+}
+
+extern "C" void apply_traces_lowpass(float **tr, float **trs, int nt, int ntr, float fpass, float fcut, float dt)
+{
+    traces_filter(tr, trs, nt, ntr, fpass, fcut, dt, 0, "apply_traces_lowpass");
+}
+
+extern "C" void apply_traces_bandpass(float **tr, float **trs, int nt, int ntr, float fpass, float fcut, float dt)
+{
+    traces_filter(tr, trs, nt, ntr, fpass, fcut, dt, 1, "apply_traces_bandpass");
+}
+
+// interpolate_traces (common.c:482-582): ntr traces of nt samples -> ns = (nt - 1) r + 1 samples
+extern "C" void interpolate_traces(float **tr, int ntr, int nt, int r, float **trs)
+{
+    std::lock_guard<std::mutex> lk(g_ops_mu);
+    if (ntr <= 0 || nt <= 0 || !tr || !trs) {
+        fprintf(stderr, "<error>: invalid input (ntr=%d, nt=%d) in function interpolate_traces!\n", ntr, nt);
+        return;
+    }
+    if (r <= 1) {
+        memcpy(trs[0], tr[0], sizeof(float) * (size_t)ntr * nt);
+        return;
+    }
+    const int ns = (nt - 1) * r + 1;
+    const size_t nb = al((size_t)nt * ntr * 4);
+    if (!ops_ready(nb + al((size_t)ns * ntr * 4)) || !blas_ready()) return;
+    float *x = (float *)g_ops.buf, *y = (float *)(g_ops.buf + nb);
+    const int ip[3] = {nt, r, ns};
+    const float *M = op_matrix("i/" + std::to_string(nt) + "/" + std::to_string(r), (size_t)ns * nt, build_interp, ip,
+                               nullptr);
+    if (!M) return;
+    cudaMemcpyAsync(x, tr[0], sizeof(float) * (size_t)nt * ntr, cudaMemcpyHostToDevice, g_ops.st);
+    const float one = 1.0f, zero = 0.0f;
+    // y[itr] = M x[itr]: each trace a column of length nt, each output a column of length ns
+    if (cublasSgemm(g_blas, CUBLAS_OP_N, CUBLAS_OP_N, ns, ntr, nt, &one, M, ns, x, nt, &zero, y, ns) !=
+        CUBLAS_STATUS_SUCCESS) {
+        fprintf(stderr, "<error>: interpolate_traces: GEMM failed\n");
+        return;
+    }
+    cudaMemcpyAsync(trs[0], y, sizeof(float) * (size_t)ns * ntr, cudaMemcpyDeviceToHost, g_ops.st);
+    report(cudaStreamSynchronize(g_ops.st), "interpolate_traces");
 }
 
 // apply_gradient_shot_precondition, optimization.c:58-97

@@ -287,3 +287,87 @@ void fwi_model_update(float *slow, float *vp, float *rho, const float *perturb, 
     }
     reciprocal(vp, slow, n);
 }
+
+/* ------------------------------------------------------------ residual filters, interpolation */
+/* The window values come from the reference's own float expressions (apply_traces_lowpass and
+ * apply_traces_bandpass; the bandpass forms its cosine argument in double because PI is a double
+ * constant there).  Only entries 0..n/2 are used (the non-negative frequencies of an r2c FFT). */
+void fwi_filter_window(int filter, int n, float fpass, float fcut, float dt, float *win)
+{
+    const float df = 1.0f / (n * dt);
+    for (int it = 0; it < n; it++) {
+        const float f = it * df;
+        if (filter == 0) {
+            const float taperLen = fcut - fpass;
+            if (f < fpass) win[it] = 1.0f;
+            else if (f >= fpass && f <= fcut)
+                win[it] = 0.5f * (1.0f + cosf((float)3.141592653589793 * (f - fpass) / taperLen));
+            else win[it] = 0.0f;
+        } else {
+            const float lo = fpass, hi = fcut - fpass;
+            if (f < fpass) win[it] = 0.5f * (1.0f + cosf(3.141592653589793 * (fpass - f) / lo));
+            else if (f >= fpass && f <= fcut) win[it] = 0.5f * (1.0f + cosf(3.141592653589793 * (f - fpass) / hi));
+            else win[it] = 0.0f;
+        }
+    }
+}
+
+/* h[m] = (1/n) sum_k W(k) cos(2 pi k m / n) with W(k) = win[min(k, n - k)] (the real window seen
+ * by a real signal's full spectrum), in double; k m mod n is stepped incrementally */
+static void circular_kernel(const float *win, int n, double *h)
+{
+    double *cs = (double *)malloc(sizeof(double) * (size_t)n);
+    for (int m = 0; m < n; m++) cs[m] = cos(2.0 * 3.141592653589793 * m / n);
+    for (int m = 0; m < n; m++) {
+        double a = 0.0;
+        int idx = 0;
+        for (int k = 0; k < n; k++) {
+            a += (double)win[k <= n / 2 ? k : n - k] * cs[idx];
+            idx += m;
+            if (idx >= n) idx -= n;
+        }
+        h[m] = a / n;
+    }
+    free(cs);
+}
+
+void fwi_filter_operator(int filter, int n, float fpass, float fcut, float dt, float *C)
+{
+    float *win = (float *)malloc(sizeof(float) * (size_t)n);
+    double *h = (double *)malloc(sizeof(double) * (size_t)n);
+    fwi_filter_window(filter, n, fpass, fcut, dt, win);
+    circular_kernel(win, n, h);
+    for (int j = 0; j < n; j++)
+        for (int i = 0; i < n; i++) C[(size_t)j * n + i] = (float)h[(i - j + n) % n];
+    free(win);
+    free(h);
+}
+
+/* zero-stuffing by r, a rectangular window of height r on |k| < N / (2r) of the length-N
+ * spectrum (N = (ns - 1) r + 1), inverse FFT, real part / N:  y[i] = sum_j x[j] g[(i - j r) mod N] */
+void fwi_interp_operator(int ns, int r, int nt, float *M)
+{
+    const int N = (ns - 1) * r + 1, nkeep = N / (2 * r);
+    float *win = (float *)calloc((size_t)N, sizeof(float));
+    for (int k = 0; k < nkeep; k++) win[k] = (float)r;
+    for (int k = N - nkeep + 1; k < N; k++) win[k] = (float)r;
+    /* win is symmetric (win[k] = win[N - k]), so g is the cosine sum of the full window */
+    double *g = (double *)malloc(sizeof(double) * (size_t)N), *cs = (double *)malloc(sizeof(double) * (size_t)N);
+    for (int m = 0; m < N; m++) cs[m] = cos(2.0 * 3.141592653589793 * m / N);
+    for (int m = 0; m < N; m++) {
+        double a = 0.0;
+        int idx = 0;
+        for (int k = 0; k < N; k++) {
+            a += (double)win[k] * cs[idx];
+            idx += m;
+            if (idx >= N) idx -= N;
+        }
+        g[m] = a / N;
+    }
+    for (int j = 0; j < ns; j++)
+        for (int i = 0; i < nt; i++)
+            M[(size_t)j * nt + i] = i < N ? (float)g[(((long long)i - (long long)j * r) % N + N) % N] : 0.0f;
+    free(win);
+    free(g);
+    free(cs);
+}

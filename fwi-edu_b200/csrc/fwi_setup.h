@@ -42,6 +42,17 @@ void fwi_model_update(float *slow, float *vp, float *rho, const float *perturb, 
 /* cosine taper coefficients 0.5(1+cos(pi*i/L)), i = 0..L (common.c:826-831) */
 void fwi_taper_coefs(int L, float *out);
 
+/* The residual filters and trace interpolation as matrices (column-major, float), so that the
+ * device applies them to all traces of all shots as one GEMM each.
+ * fwi_filter_operator: apply_traces_lowpass (filter 0, common.c:584-687) or apply_traces_bandpass
+ *   (filter 1, :689-794) of length-n traces: FFT, the cosine-tapered window on the non-negative
+ *   frequencies, inverse FFT, / n -- a circular convolution, C[i + j n] = h[(i - j) mod n].
+ * fwi_interp_operator: interpolate_traces (:482-582) from ns to nt samples by r: M[i + j nt],
+ *   rows i >= (ns - 1) r + 1 zero. */
+void fwi_filter_window(int filter, int n, float fpass, float fcut, float dt, float *win);
+void fwi_filter_operator(int filter, int n, float fpass, float fcut, float dt, float *C);
+void fwi_interp_operator(int ns, int r, int nt, float *M);
+
 #ifdef __cplusplus
 }
 #endif

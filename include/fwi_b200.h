@@ -111,6 +111,15 @@ FWI_API void alloc_acoustic2dCheckPoint(Acoustic2dCheckPoint *chkpt, int NZ, int
 FWI_API void free_acoustic2dCheckPoint(Acoustic2dCheckPoint *chkpt);
 FWI_API float calculate_memory_cost_checkpoint(int nt, int NX, int NZ);
 
+/* common.c:584-687 / :689-794 / :482-582 (common.h): the residual filters (FFT, cosine-tapered
+ * low/band-pass window, inverse FFT, / nt) of ntr traces of nt samples, and the interpolation
+ * of ntr traces from nt to (nt - 1) r + 1 samples (zero-stuffing, rectangular band window).
+ * Arrays in the alloc2float layout.  On the GPU as GEMMs with the equivalent operator matrices
+ * (FP32 within 1e-6 relative of the transforms). */
+FWI_API void apply_traces_lowpass(float **tr, float **trs, int nt, int ntr, float fpass, float fcut, float dt);
+FWI_API void apply_traces_bandpass(float **tr, float **trs, int nt, int ntr, float fpass, float fcut, float dt);
+FWI_API void interpolate_traces(float **tr, int ntr, int nt, int r, float **trs);
+
 /* replace the optimization.h reductions (optimization.c:13-298), computed on the device */
 FWI_API void apply_gradient_precondition(float *grad, const float *precond, int n, float alpha);
 FWI_API void apply_gradient_shot_precondition(float *grad, float *precond, int n);

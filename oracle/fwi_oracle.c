@@ -498,7 +498,60 @@ static void adjoint_taper_lengths(const OrcShot *s, const float *vp_global, int 
     *ltrace = (int)roundf((2.0f / kpass) / s->dtr) + 1;
 }
 
-/* compute_adjoint_source2d, optimization.c:300-419 (filter 2: residual and tapers) */
+/* The cosine-tapered spectral windows of apply_traces_lowpass (common.c:584-687, filter 0)
+ * and apply_traces_bandpass (common.c:689-794, filter 1), with the reference's float
+ * expressions (PI is CWP's double constant: the bandpass argument is formed in double). */
+static void filter_window(int filter, int n, float fpass, float fcut, float dt, float *win)
+{
+    float df = 1.0f / (n * dt);
+    for (int it = 0; it < n; it++) {
+        float f = it * df;
+        if (filter == 0) {
+            float taperLen = fcut - fpass;
+            if (f < fpass) win[it] = 1.0f;
+            else if (f >= fpass && f <= fcut) win[it] = 0.5f * (1.0f + cosf((float)3.141592653589793 * (f - fpass) / taperLen));
+            else win[it] = 0.0f;
+        } else {
+            float lo = fpass, hi = fcut - fpass;
+            if (f < fpass) win[it] = 0.5f * (1.0f + cosf(3.141592653589793 * (fpass - f) / lo));
+            else if (f >= fpass && f <= fcut) win[it] = 0.5f * (1.0f + cosf(3.141592653589793 * (f - fpass) / hi));
+            else win[it] = 0.0f;
+        }
+    }
+}
+
+/* The filter is FFT(real) -> window on the non-negative frequencies -> inverse FFT / n, i.e. a
+ * circular convolution with h = IDFT(W_h) / n, W_h the window extended symmetrically.  Restated
+ * as that convolution, h and the sums in double (the published operation; the reference's FFTW
+ * rounding differs by ~1e-7 relative). tr: ntr traces of n samples, in place. */
+static void filter_traces(real *tr, int n, int ntr, int filter, float fpass, float fcut, float dt)
+{
+    float *win = malloc(sizeof(float) * n);
+    filter_window(filter, n, fpass, fcut, dt, win);
+    double *cs = malloc(sizeof(double) * n), *h = malloc(sizeof(double) * n), *x = malloc(sizeof(double) * n);
+    for (int m = 0; m < n; m++) cs[m] = cos(2.0 * 3.141592653589793 * m / n);
+    for (int m = 0; m < n; m++) {
+        double a = 0.0;
+        for (int k = 0; k < n; k++) {
+            int kk = k <= n / 2 ? k : n - k;
+            a += (double)win[kk] * cs[(int)(((long long)k * m) % n)];
+        }
+        h[m] = a / n;
+    }
+    for (int itr = 0; itr < ntr; itr++) {
+        real *t = tr + (size_t)itr * n;
+        for (int i = 0; i < n; i++) x[i] = t[i];
+        for (int j = 0; j < n; j++) {
+            double a = 0.0;
+            for (int i = 0; i < n; i++) a += h[(j - i + n) % n] * x[i];
+            t[j] = (real)a;
+        }
+    }
+    free(win); free(cs); free(h); free(x);
+}
+
+/* compute_adjoint_source2d, optimization.c:300-419: residual, then for filters 0/1 the time
+ * taper, time filter, trace taper and trace (wavenumber) filter, then both tapers */
 static int adjoint_source_real(const OrcShot *s, const float *vp_global, int nz, float freq, int filter,
                                const real *pre, const float *obs, real *adj)
 {
@@ -506,7 +559,23 @@ static int adjoint_source_real(const OrcShot *s, const float *vp_global, int nz,
     for (size_t i = 0; i < n; i++) adj[i] = pre[i] - (real)obs[i];
     int lt, lr;
     adjoint_taper_lengths(s, vp_global, nz, freq, &lt, &lr);
-    if (filter == 0 || filter == 1) return -1; /* FFT residual filters: not restated here */
+    if (filter == 0 || filter == 1) {
+        double vp_sum = 0.0;
+        for (int itr = 0; itr < s->ntr; itr++) vp_sum += vp_global[IDX(s->igx[itr], s->igz[itr], nz)];
+        float vp_avg = (float)(vp_sum / s->ntr);
+        float f = freq == 0.0f ? s->fpeak : freq;
+        float kpass = f / vp_avg;
+        taper_real(adj, s->ns, s->ntr, lt, 0);
+        filter_traces(adj, s->ns, s->ntr, filter, f, 2.0f * f, s->dt);
+        taper_real(adj, s->ns, s->ntr, 0, lr);
+        real *tp = malloc(sizeof(real) * n);  /* [ns][ntr]: one vector over the traces per sample */
+        for (int itr = 0; itr < s->ntr; itr++)
+            for (int it = 0; it < s->ns; it++) tp[(size_t)it * s->ntr + itr] = adj[(size_t)itr * s->ns + it];
+        filter_traces(tp, s->ntr, s->ns, filter, kpass, 2.0f * kpass, s->dtr);
+        for (int itr = 0; itr < s->ntr; itr++)
+            for (int it = 0; it < s->ns; it++) adj[(size_t)itr * s->ns + it] = tp[(size_t)it * s->ntr + itr];
+        free(tp);
+    }
     taper_real(adj, s->ns, s->ntr, lt, lr);
     return 0;
 }
@@ -605,11 +674,40 @@ int orc_forward(const OrcShot *s, const float *vpm, const float *rhom, int nz, i
 }
 
 /* interpolate_traces with r <= 1 is a copy (common.c:511-516) */
+/* interpolate_traces, common.c:482-582: zero-stuffing by r, a rectangular window of height r
+ * over |k| < N/(2r) of the length-N spectrum (N = (ns-1)r+1), inverse transform, real part / N.
+ * Restated as y[i] = sum_j x[j] g[(i - jr) mod N] with g = IDFT(window) / N in double.  Samples
+ * beyond N (when N < nt) are zero.  r <= 1 copies. */
 static int interp_traces(const real *tr, int ntr, int ns, int r, int nt, real *out)
 {
-    if (r > 1) return -1; /* FFT interpolation: not restated here */
-    for (int itr = 0; itr < ntr; itr++)
-        memcpy(out + (size_t)itr * nt, tr + (size_t)itr * ns, sizeof(real) * (size_t)ns);
+    memset(out, 0, sizeof(real) * (size_t)ntr * nt);
+    if (r <= 1) {
+        for (int itr = 0; itr < ntr; itr++)
+            memcpy(out + (size_t)itr * nt, tr + (size_t)itr * ns, sizeof(real) * (size_t)ns);
+        return 0;
+    }
+    const int N = (ns - 1) * r + 1, nkeep = N / (2 * r);
+    double *g = malloc(sizeof(double) * N), *cs = malloc(sizeof(double) * N);
+    for (int m = 0; m < N; m++) cs[m] = cos(2.0 * 3.141592653589793 * m / N);
+    for (int m = 0; m < N; m++) {
+        double a = 0.0;
+        for (int k = 0; k < N; k++) {
+            const int in_band = k < nkeep || k >= N - nkeep + 1;
+            if (in_band) a += (double)r * cs[(int)(((long long)k * m) % N)];
+        }
+        g[m] = a / N;
+    }
+    const int nout = N < nt ? N : nt;
+    for (int itr = 0; itr < ntr; itr++) {
+        const real *x = tr + (size_t)itr * ns;
+        real *y = out + (size_t)itr * nt;
+        for (int i = 0; i < nout; i++) {
+            double a = 0.0;
+            for (int j = 0; j < ns; j++) a += g[((i - j * r) % N + N) % N] * (double)x[j];
+            y[i] = (real)a;
+        }
+    }
+    free(g); free(cs);
     return 0;
 }
 
@@ -621,7 +719,7 @@ static int shot_gradient_real(const OrcShot *s, const float *vp, const float *rh
     int nxx = s->ix_max - s->ix_min + 1;
     int rc = check_shot(s, nt, nz, nxx, pml, fs);
     if (rc) return rc;
-    if (s->sampleRate > 1 || filter == 0 || filter == 1) return -10;
+    if (filter < 0 || filter > 2) return -10;
     float *vpw = malloc(sizeof(float) * (size_t)nz * nxx), *rhow = malloc(sizeof(float) * (size_t)nz * nxx);
     window_model(vp, nz, s->ix_min, nxx, vpw);
     window_model(rho, nz, s->ix_min, nxx, rhow);

@@ -9,7 +9,7 @@ calculate_peak_frequency) on small seeded cases and stores inputs and outputs as
 compressed .npz files.  The reference checkout is needed only here; the fixtures
 travel with the repository.
 
-    OMP_NUM_THREADS=1 python tests/golden/make_golden.py
+    OMP_NUM_THREADS=1 python tests/golden/make_golden.py [case ...]
 """
 from __future__ import annotations
 
@@ -55,7 +55,7 @@ def pack_shots(shots):
 
 
 def case(name, nz, nx, nt, dt, pml, fs, nshot, seed, problems=(0, 1, 2), precondition=1, sr=1, obs_src_depth=None,
-         **kw):
+         filt=2.0, **kw):
     ref = po.Reference("strict")
     vp = M.layered_model(nz, nx, seed=seed, water_rows=6, anom_sigma=4)
     rho = M.gardner(vp, water_rows=6)
@@ -66,7 +66,7 @@ def case(name, nz, nx, nt, dt, pml, fs, nshot, seed, problems=(0, 1, 2), precond
             s.ns = (nt - 1) // sr + 1
             s.dt = float(np.float32(np.float32(dt) * sr))
     out = dict(vp=vp, rho=rho, nz=nz, nx=nx, nt=nt, dt=np.float32(dt), dx=np.float32(DX), pml=pml, fs=fs,
-               precondition=precondition, nshot=nshot)
+               precondition=precondition, nshot=nshot, filter=np.float32(filt))
     out.update(pack_shots(shots))
     out["fpeak_ref"] = np.float32(ref.peak_frequency(shots[0].src, nt, dt))
     obs_shots = shots
@@ -82,7 +82,7 @@ def case(name, nz, nx, nt, dt, pml, fs, nshot, seed, problems=(0, 1, 2), precond
         rho0 = M.gardner(vp0, water_rows=6)
         out["vp0"], out["rho0"] = vp0, rho0
         freq = 10.0
-        adj, grad = ref.propagation(vp0, rho0, shots, DX, DX, dt, nt, pml, fs, freq, 2.0, precondition, 1, obs=obs)
+        adj, grad = ref.propagation(vp0, rho0, shots, DX, DX, dt, nt, pml, fs, freq, filt, precondition, 1, obs=obs)
         for i, t in enumerate(adj):
             out[f"adj{i}"] = t
         out["grad"] = grad
@@ -101,7 +101,7 @@ def case(name, nz, nx, nt, dt, pml, fs, nshot, seed, problems=(0, 1, 2), precond
         rho1 = M.gardner(vp1, water_rows=6)
         out["vp1"], out["rho1"] = vp1, rho1
         if 2 in problems:
-            res, _ = ref.propagation(vp1, rho1, shots, DX, DX, dt, nt, pml, fs, freq, 2.0, precondition, 2, obs=obs)
+            res, _ = ref.propagation(vp1, rho1, shots, DX, DX, dt, nt, pml, fs, freq, filt, precondition, 2, obs=obs)
             for i, t in enumerate(res):
                 out[f"res{i}"] = t
             out["fun2"] = np.float32(ref.objective(res, shots))
@@ -117,6 +117,11 @@ def main():
     if not po.ref_available("strict"):
         if not po.build_ref():
             raise SystemExit("the reference checkout is needed to regenerate the golden vectors")
+    only = set(sys.argv[1:])
+    if only:  # regenerate the named cases only
+        global case
+        full = case
+        case = lambda name, *a, **k: full(name, *a, **k) if name in only else None  # noqa: E731
     case("fs1_small", 40, 70, 300, 0.001, 8, 1, 3, seed=3)
     case("fs0_small", 40, 70, 300, 0.001, 8, 0, 3, seed=4)
     # nt = 200 gives d = 20 with nt % d == 0: the last segment replays d-1 steps
@@ -128,6 +133,13 @@ def main():
     case("fs1_edges", 36, 52, 240, 0.001, 5, 1, 2, seed=6, dup=True, src_depth=0, obs_src_depth=1, precondition=0)
     case("noprec", 36, 60, 220, 0.001, 7, 1, 2, seed=7, precondition=0)
     case("sr2_fwd", 36, 60, 301, 0.001, 7, 1, 2, seed=8, problems=(0,), sr=2)
+    # FFT residual filters (optimization.c:368-415): lowpass and bandpass in time and space
+    case("filt0", 40, 70, 300, 0.001, 8, 1, 3, seed=9, filt=0.0)
+    case("filt1", 40, 70, 300, 0.001, 8, 1, 2, seed=10, problems=(0, 1), filt=1.0)
+    # observed data every 2nd step: the adjoint source is interpolated back to every step
+    # (interpolate_traces, common.c:482-582), with and without the lowpass
+    case("sr2_grad", 36, 60, 301, 0.001, 7, 1, 2, seed=11, sr=2)
+    case("sr2_filt0", 36, 60, 301, 0.001, 7, 1, 2, seed=12, problems=(0, 1), sr=2, filt=0.0)
 
 
 if __name__ == "__main__":

@@ -34,6 +34,11 @@ class Case:
                                    sampleRate=sr, ix_min=ixmin, ix_max=ixmax, dt=dt, dtr=dtr, fpeak=fpeak, src=src,
                                    sx=sx, sz=sz))
         self.obs = [z[f"obs{i}"] for i in range(self.nshot)]
+        # residual filter of the gradient case (optimization.c:368-415) and whether an FFT stage
+        # (filters 0/1, or interpolation for sampleRate > 1) lies between the forward traces and
+        # the adjoint source: those results are compared within a tolerance, the rest bit for bit
+        self.filter = float(z["filter"]) if "filter" in z else 2.0
+        self.fft = int(self.filter) in (0, 1) or any(s.sampleRate > 1 for s in self.shots)
         self.has_grad = "grad" in z
         if self.has_grad:
             self.vp0, self.rho0 = z["vp0"], z["rho0"]

@@ -3,7 +3,11 @@
 The golden vectors were produced by the unmodified FWI-EDU C sources (strict IEEE
 build, one OpenMP thread; tests/golden/make_golden.py).  The FP32 restatement must
 reproduce every one of them bit for bit before it may serve as the checker of the
-CUDA engine.
+CUDA engine -- except where an FFT stands between the forward traces and the adjoint
+source (residual filters 0/1, interpolation of sampleRate > 1 records): the reference
+runs FFTW-style transforms there, the restatement the same linear operator as an
+explicit convolution in double, so those results agree within stated tolerances
+(adjoint sources and residuals rel-L2 <= 1e-5, gradients <= 1e-4).
 """
 import numpy as np
 import pytest
@@ -24,10 +28,16 @@ def test_forward_traces_bitexact(port32, name):
         assert np.array_equal(pre[i], c.obs[i]), f"shot {i}"
 
 
-@pytest.mark.parametrize("name", [n for n in CASES if Case(n).has_grad])
+def rel(a, b):
+    a = np.asarray(a, np.float64)
+    b = np.asarray(b, np.float64)
+    return float(np.linalg.norm(a - b) / max(np.linalg.norm(b), 1e-300))
+
+
+@pytest.mark.parametrize("name", [n for n in CASES if Case(n).has_grad and not Case(n).fft])
 def test_gradient_and_adjoint_source_bitexact(port32, name):
     c = Case(name)
-    adj, grad = port32.propagation(c.vp0, c.rho0, c.shots, c.dx, c.dx, c.dt, c.nt, c.pml, c.fs, 10.0, 2.0,
+    adj, grad = port32.propagation(c.vp0, c.rho0, c.shots, c.dx, c.dx, c.dt, c.nt, c.pml, c.fs, 10.0, c.filter,
                                    c.precondition, 1, obs=c.obs)
     for i in range(c.nshot):
         assert np.array_equal(adj[i], c.adj[i]), f"adjoint source, shot {i}"
@@ -35,16 +45,34 @@ def test_gradient_and_adjoint_source_bitexact(port32, name):
     assert np.isfinite(grad).all() and np.abs(grad).max() > 0
 
 
-@pytest.mark.parametrize("name", [n for n in CASES if Case(n).has_grad and Case(n).has_res])
+@pytest.mark.parametrize("name", [n for n in CASES if Case(n).has_grad and Case(n).has_res and not Case(n).fft])
 def test_line_search_residual_bitexact(port32, name):
     c = Case(name)
-    res, _ = port32.propagation(c.vp1, c.rho1, c.shots, c.dx, c.dx, c.dt, c.nt, c.pml, c.fs, 10.0, 2.0,
+    res, _ = port32.propagation(c.vp1, c.rho1, c.shots, c.dx, c.dx, c.dt, c.nt, c.pml, c.fs, 10.0, c.filter,
                                 c.precondition, 2, obs=c.obs)
     for i in range(c.nshot):
         assert np.array_equal(res[i], c.res[i]), f"shot {i}"
     assert port32.objective(c.adj) == float(c["fun1"])
     assert port32.objective(c.res) == float(c["fun2"])
     assert port32.step_length(c.adj, c.res) == float(c["steplen"])
+
+
+@pytest.mark.parametrize("name", [n for n in CASES if Case(n).has_grad and Case(n).fft])
+def test_filtered_and_interpolated_gradient(port32, name):
+    """Filters 0/1 and sampleRate > 1: the FFT stages within tolerance, the rest unchanged."""
+    c = Case(name)
+    adj, grad = port32.propagation(c.vp0, c.rho0, c.shots, c.dx, c.dx, c.dt, c.nt, c.pml, c.fs, 10.0, c.filter,
+                                   c.precondition, 1, obs=c.obs)
+    for i in range(c.nshot):
+        assert rel(adj[i], c.adj[i]) <= 1e-5, f"adjoint source, shot {i}: {rel(adj[i], c.adj[i]):.2e}"
+    assert rel(grad, c.grad) <= 1e-4, f"gradient {rel(grad, c.grad):.2e}"
+    if c.has_res:
+        res, _ = port32.propagation(c.vp1, c.rho1, c.shots, c.dx, c.dx, c.dt, c.nt, c.pml, c.fs, 10.0, c.filter,
+                                    c.precondition, 2, obs=c.obs)
+        for i in range(c.nshot):
+            assert rel(res[i], c.res[i]) <= 1e-5, f"residual, shot {i}"
+        assert abs(port32.objective(c.res) - float(c["fun2"])) <= 1e-5 * abs(float(c["fun2"]))
+        assert abs(port32.step_length(c.adj, c.res) - float(c["steplen"])) <= 1e-5 * abs(float(c["steplen"]))
 
 
 @pytest.mark.parametrize("name", [n for n in CASES if Case(n).has_grad])
