@@ -30,6 +30,7 @@
 #include <map>
 #include <memory>
 #include <mutex>
+#include <set>
 #include <string>
 #include <vector>
 
@@ -135,7 +136,10 @@ struct fwi_ctx {
     std::map<std::string, cudaGraphExec_t> graphs;
     fwi_stats stats{};
     int math = 0;  // 0: bit-exact arithmetic, 1: contracted multiply-adds
+    bool use_graphs = true;  // capture the batched launch sequences as CUDA graphs
     int *d_err = nullptr;  // set by a step kernel whose tile copy did not complete
+    std::map<void *, size_t> sizes;  // live device blocks of this context
+    size_t peak = 0;
     // exchange hook of a shot-sharded run (one context per GPU): sums device doubles over ranks
     fwi_allreduce_fn ar_fn = nullptr;
     void *ar_user = nullptr;
@@ -158,28 +162,37 @@ struct fwi_ctx {
     double last_obj = 0.0;
 };
 
+// Device memory comes from the stream-ordered allocator on the context's stream: a context
+// that frees or grows its state never synchronises the device, so contexts on other streams
+// (concurrent requests of a server) keep running.  Every block's size is tracked for the budget.
 static int dmalloc(fwi_ctx *c, void **p, size_t bytes)
 {
     if (c->budget && c->used + bytes > c->budget)
         return fail(FWI_ERR_NOMEM, "device budget exceeded: %zu + %zu > %zu bytes", c->used, bytes, c->budget);
-    cudaError_t e = cudaMalloc(p, bytes ? bytes : 16);
-    if (e != cudaSuccess) return fail(FWI_ERR_NOMEM, "cudaMalloc(%zu): %s", bytes, cudaGetErrorString(e));
+    cudaError_t e = cudaMallocAsync(p, bytes ? bytes : 16, c->stream);
+    if (e != cudaSuccess) return fail(FWI_ERR_NOMEM, "cudaMallocAsync(%zu): %s", bytes, cudaGetErrorString(e));
+    e = cudaStreamSynchronize(c->stream);  // usable from any stream and from synchronous copies
+    if (e != cudaSuccess) return fail(FWI_ERR_CUDA, "cudaStreamSynchronize: %s", cudaGetErrorString(e));
+    c->sizes[*p] = bytes;
     c->used += bytes;
+    c->peak = std::max(c->peak, c->used);
     return FWI_OK;
 }
-static void dfree(fwi_ctx *c, void *p, size_t bytes)
+static void dfree(fwi_ctx *c, void *p, size_t = 0)
 {
-    if (p) {
-        cudaFree(p);
-        c->used -= std::min(c->used, bytes);
+    if (!p) return;
+    auto it = c->sizes.find(p);
+    if (it != c->sizes.end()) {
+        c->used -= std::min(c->used, it->second);
+        c->sizes.erase(it);
     }
+    cudaFreeAsync(p, c->stream);
 }
 
 static void free_run(fwi_ctx *c, ShotRun *r)
 {
-    for (void *p : r->allocs) cudaFree(p);
+    for (void *p : r->allocs) dfree(c, p);
     r->allocs.clear();
-    (void)c;
 }
 
 static void drop_graphs(fwi_ctx *c)
@@ -209,10 +222,11 @@ extern "C" int fwi_ctx_create(fwi_ctx **out, int device, size_t budget)
     c->device = device;
     c->budget = budget;
     if (const char *e = getenv("FWI_MATH")) c->math = atoi(e) ? 1 : 0;
+    if (const char *e = getenv("FWI_GRAPH")) c->use_graphs = e[0] != '0';  // 0: direct launches (profilers)
     CK(cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking));
     CK(cudaEventCreate(&c->ev0));
     CK(cudaEventCreate(&c->ev1));
-    CK(cudaMalloc((void **)&c->d_err, sizeof(int)));
+    TRY(dmalloc(c, (void **)&c->d_err, sizeof(int)));
     CK(cudaMemset(c->d_err, 0, sizeof(int)));
     *out = c;
     return FWI_OK;
@@ -224,19 +238,12 @@ extern "C" int fwi_ctx_destroy(fwi_ctx *c)
     cudaSetDevice(c->device);
     cudaStreamSynchronize(c->stream);
     free_runs(c);
-    for (auto &kv : c->progs) cudaFree(kv.second.d);
-    for (auto &p : c->plans) {
-        cudaFree(p->d_coef);
-        fwi_free_coefs(&p->hc);
-    }
-    for (float *p : c->d_obs) cudaFree(p);
-    for (float *p : c->d_pre) cudaFree(p);
-    for (float *p : c->d_pre_alt) cudaFree(p);
-    cudaFree(c->d_vp); cudaFree(c->d_rho); cudaFree(c->d_grad); cudaFree(c->d_prec);
-    cudaFree(c->d_gc); cudaFree(c->d_red); cudaFree(c->d_scratch); cudaFree(c->d_desc);
-    cudaFree(c->d_err); cudaFree(c->d_xchg); cudaFree(c->d_fft_tmp);
-    for (auto &kv : c->ops) cudaFree(kv.second.first);
+    for (auto &p : c->plans) fwi_free_coefs(&p->hc);
+    // everything left in the allocator table belongs to this context
+    for (auto &kv : c->sizes) cudaFreeAsync(kv.first, c->stream);
+    c->sizes.clear();
     if (c->blas) cublasDestroy(c->blas);
+    cudaStreamSynchronize(c->stream);
     cudaEventDestroy(c->ev0); cudaEventDestroy(c->ev1);
     cudaStreamDestroy(c->stream);
     delete c;
@@ -253,10 +260,10 @@ static int set_model_common(fwi_ctx *c, int nz, int nx, float dx, float dz, floa
                 dz == c->dz && dt == c->dt;
     if (!same) {
         free_runs(c);
-        for (auto &kv : c->progs) cudaFree(kv.second.d);
+        for (auto &kv : c->progs) dfree(c, kv.second.d);
         c->progs.clear();
         for (auto &p : c->plans) {
-            cudaFree(p->d_coef);
+            dfree(c, p->d_coef);
             fwi_free_coefs(&p->hc);
         }
         c->plans.clear();
@@ -1266,8 +1273,7 @@ static int run_program(fwi_ctx *c, const std::string &key, const Program *prog, 
                        const ShotRun *r0, bool batched)
 {
     if (!batched) return launch_steps(c, prog, shot_base, nshot, r0, false);
-    const char *ge = getenv("FWI_GRAPH");  // FWI_GRAPH=0: issue the launches directly (profilers, debugging)
-    if (ge && ge[0] == '0') return launch_steps(c, prog, shot_base, nshot, r0, true);
+    if (!c->use_graphs) return launch_steps(c, prog, shot_base, nshot, r0, true);
     auto it = c->graphs.find(key);
     if (it == c->graphs.end()) {
         cudaGraph_t g;
@@ -1502,6 +1508,52 @@ extern "C" int fwi_ctx_objective(fwi_ctx *c, double *out)
     TRY(exchange_scalars(c, &acc, 1));
     *out = 0.5 * acc;
     return FWI_OK;
+}
+
+extern "C" int fwi_ctx_set_graphs(fwi_ctx *c, int on)
+{
+    if (!c) return fail(FWI_ERR_ARG, "ctx is NULL");
+    if (!on) drop_graphs(c);
+    c->use_graphs = on != 0;
+    return FWI_OK;
+}
+
+// Device bytes a context needs for one run of `problem` over these shots: the allocations of
+// set_model / set_shots / prepare_run / assign_pool / the FFT stage, with a margin for the
+// reduction, descriptor and library workspaces.  A serving loop admits requests by it.
+extern "C" size_t fwi_estimate_bytes(const fwi_shot *shots, int nshot, int nz, int nx, int nt, int pml, int problem,
+                                     int filter)
+{
+    if (!shots || nshot <= 0 || nz <= 0 || nx <= 0 || nt <= 0 || pml < 0) return 0;
+    const size_t m = (size_t)nz * nx;
+    size_t b = 4 * m * 4 + 2 * m * 8;  // vp, rho, grad, prec; FP64 stacks of g and H
+    const bool grad = problem == 1;
+    const int d = fwi_ck_interval(nt), K = (nt - 1) / d, S5 = d / MST + 2;
+    std::set<std::pair<int, int>> windows;
+    size_t max_ns = 1, max_ntr = 1;
+    for (int i = 0; i < nshot; i++) {
+        const fwi_shot &s = shots[i];
+        const int nxx = s.ix_max - s.ix_min + 1;
+        const size_t Nx = (size_t)nxx + 2 * pml, Nz = (size_t)nz + 2 * pml, ld = (Nz + 3) / 4 * 4;
+        const size_t frame = Nx * ld, rec = (size_t)s.ntr * s.ns;
+        windows.insert({s.ix_min, s.ix_max});
+        b += 3 * rec * 4;                                                // observed, predicted, line-search gathers
+        b += (size_t)nt * 12 + (Nx + 1) * 4 + (size_t)s.ntr * 16 + rec * 4;  // source terms, receivers, samples
+        b += ((size_t)s.ns + 1 + s.ntr + 1) * 4;                         // taper coefficients
+        b += (grad ? (size_t)nframes_gradient(K, S5) : 3) * frame * 4;   // frame block in the pool
+        if (grad) b += 2 * frame * 8 + (size_t)nt * s.ntr * 4 + 2 * (size_t)nz * nxx * 4;
+        max_ns = std::max(max_ns, (size_t)s.ns);
+        max_ntr = std::max(max_ntr, (size_t)s.ntr);
+    }
+    for (auto &w : windows) {
+        const size_t Nx = (size_t)(w.second - w.first + 1) + 2 * pml, Nz = (size_t)nz + 2 * pml;
+        b += 6 * Nx * ((Nz + 3) / 4 * 4) * 4;  // coefficient planes of the window
+    }
+    if ((grad || problem == 2) && (filter == 0 || filter == 1))
+        b += max_ns * max_ntr * 4 + max_ns * max_ns * 4 + (size_t)nshot * max_ntr * max_ntr * 4;
+    if (grad) b += (size_t)nt * max_ns * 4;  // interpolation operator (sampleRate > 1)
+    b += (size_t)nshot * sizeof(ShotDesc) + ((size_t)3 * nt + 64) * sizeof(int4) + (8u << 20);
+    return b + b / 20 + (96u << 20);  // 5 % and 96 MiB for the library workspaces and graphs
 }
 
 extern "C" int fwi_adjoint_program(int nt, int overlap, int *items, int cap)

@@ -289,3 +289,129 @@ class Context:
         s = FwiStats()
         _check(self.L.fwi_ctx_stats(self.h, C.byref(s)))
         return {k: getattr(s, k) for k, _ in FwiStats._fields_}
+
+
+# ---------------------------------------------------------------- serving (fwi_server_*)
+REQ_MODEL, REQ_GRADIENT = 0, 1
+REQ_QUEUED, REQ_RUNNING, REQ_DONE, REQ_FAILED = range(4)
+
+
+class FwiRequest(C.Structure):
+    _fields_ = [("kind", C.c_int), ("nz", C.c_int), ("nx", C.c_int), ("dx", C.c_float), ("dz", C.c_float),
+                ("dt", C.c_float), ("nt", C.c_int), ("pml", C.c_int), ("fs", C.c_int), ("vp", _fp), ("rho", _fp),
+                ("shots", C.POINTER(FwiShot)), ("nshot", C.c_int), ("obs", _fpp), ("freq", C.c_float),
+                ("filter", C.c_int), ("precondition", C.c_int), ("traces", _fpp), ("grad", _fp)]
+
+
+class RequestInfo(C.Structure):
+    _fields_ = [("state", C.c_int), ("status", C.c_int), ("bytes", C.c_size_t), ("queue_ms", C.c_double),
+                ("run_ms", C.c_double), ("total_ms", C.c_double), ("objective", C.c_double),
+                ("cell_updates", C.c_double), ("error", C.c_char * 256)]
+
+
+class ServerReport(C.Structure):
+    _fields_ = [("submitted", C.c_longlong), ("completed", C.c_longlong), ("failed", C.c_longlong),
+                ("rejected", C.c_longlong), ("p50_ms", C.c_double), ("p99_ms", C.c_double), ("max_ms", C.c_double),
+                ("p50_queue_ms", C.c_double), ("p99_queue_ms", C.c_double), ("wall_s", C.c_double),
+                ("cell_updates", C.c_double), ("shots_modeled", C.c_double), ("shot_gradients", C.c_double),
+                ("budget", C.c_size_t), ("peak_bytes", C.c_size_t), ("max_active", C.c_int),
+                ("peak_active", C.c_int)]
+
+
+def _shot_array(shots, keep):
+    arr = (FwiShot * len(shots))()
+    for i, s in enumerate(shots):
+        igx, igz, src = _i32(s.igx), _i32(s.igz), _f32(s.src)
+        keep += [igx, igz, src]
+        a = arr[i]
+        a.shotID = s.shotID; a.isx = s.isx; a.isz = s.isz; a.ntr = len(igx); a.ns = s.ns
+        a.sampleRate = s.sampleRate; a.ix_min = s.ix_min; a.ix_max = s.ix_max
+        a.dt = s.dt; a.dtr = s.dtr; a.fpeak = s.fpeak
+        a.src = _ptr(src); a.igx = _ptr(igx, _ip); a.igz = _ptr(igz, _ip)
+    keep.append(arr)
+    return arr
+
+
+def request(kind, vp, rho, dx, dz, dt, nt, pml, fs, shots, obs=None, freq=10.0, filt=2, precondition=1):
+    """A fwi_request with its input and output buffers (kept in the returned holder):
+    returns (FwiRequest, holder) where holder["traces"] / holder["grad"] receive the results."""
+    keep = []
+    vp, rho = _f32(vp), _f32(rho)
+    nx, nz = vp.shape
+    keep += [vp, rho]
+    r = FwiRequest()
+    r.kind = kind; r.nz = nz; r.nx = nx; r.dx = dx; r.dz = dz; r.dt = dt; r.nt = nt; r.pml = pml; r.fs = fs
+    r.vp = _ptr(vp); r.rho = _ptr(rho)
+    r.shots = C.cast(_shot_array(shots, keep), C.POINTER(FwiShot)); r.nshot = len(shots)
+    if obs is not None:
+        obs = [_f32(o) for o in obs]
+        keep += obs
+        po = (_fp * len(obs))(*[_ptr(o) for o in obs])
+        keep.append(po)
+        r.obs = C.cast(po, _fpp)
+    r.freq = freq; r.filter = filt; r.precondition = precondition
+    traces = [np.zeros((len(s.igx), s.ns), np.float32) for s in shots]
+    pt = (_fp * len(traces))(*[_ptr(t) for t in traces])
+    keep += [traces, pt]
+    r.traces = C.cast(pt, _fpp)
+    grad = np.zeros((nx, nz), np.float32) if kind == REQ_GRADIENT else None
+    if grad is not None:
+        r.grad = _ptr(grad)
+    keep.append(r)
+    return r, {"traces": traces, "grad": grad, "keep": keep}
+
+
+class Server:
+    """The serving loop (fwi_server_*): concurrent, footprint-admitted requests on one GPU."""
+
+    def __init__(self, device=0, budget_bytes=0, max_active=4):
+        self.L = lib()
+        self.L.fwi_request_bytes.restype = C.c_size_t
+        self.L.fwi_estimate_bytes.restype = C.c_size_t
+        self.h = C.c_void_p()
+        _check(self.L.fwi_server_create(C.byref(self.h), device, C.c_size_t(budget_bytes), max_active))
+        self.pending = {}
+
+    def bytes(self, req):
+        return int(self.L.fwi_request_bytes(C.byref(req)))
+
+    def submit(self, req, holder):
+        rid = C.c_longlong()
+        _check(self.L.fwi_server_submit(self.h, C.byref(req), C.byref(rid)))
+        self.pending[rid.value] = holder
+        return rid.value
+
+    def wait(self, rid, timeout_s=-1.0):
+        info = RequestInfo()
+        rc = self.L.fwi_server_wait(self.h, C.c_longlong(rid), C.c_double(timeout_s), C.byref(info))
+        out = {k: getattr(info, k) for k, _ in RequestInfo._fields_}
+        out["error"] = info.error.decode(errors="replace")
+        if rc == FWI_OK:
+            holder = self.pending.pop(rid)
+            out["traces"], out["grad"] = holder["traces"], holder["grad"]
+        return out
+
+    def report(self):
+        s = ServerReport()
+        _check(self.L.fwi_server_stats(self.h, C.byref(s)))
+        return {k: getattr(s, k) for k, _ in ServerReport._fields_}
+
+    def close(self):
+        if self.h:
+            self.L.fwi_server_destroy(self.h)
+            self.h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def estimate_bytes(shots, nz, nx, nt, pml, problem, filt=2):
+    """fwi_estimate_bytes: device bytes one context needs for the run (host-side, no GPU)."""
+    L = lib()
+    L.fwi_estimate_bytes.restype = C.c_size_t
+    keep = []
+    arr = _shot_array(shots, keep)
+    return int(L.fwi_estimate_bytes(arr, len(shots), nz, nx, nt, pml, problem, filt))

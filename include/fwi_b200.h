@@ -188,6 +188,65 @@ typedef struct {
 } fwi_stats;
 FWI_API int fwi_ctx_stats(fwi_ctx *ctx, fwi_stats *out);
 
+/* CUDA graphs on the batched path (default on; FWI_GRAPH=0 in the environment turns them off):
+ * off, every step is launched directly -- cheaper for a launch sequence run only once. */
+FWI_API int fwi_ctx_set_graphs(fwi_ctx *ctx, int on);
+
+/* Device bytes a context needs for one run of `problem` (0 modeling, 1 gradient, 2 line-search
+ * residual) over these shots of an nz x nx model: what a serving loop admits requests by.
+ * No counterpart in the reference. */
+FWI_API size_t fwi_estimate_bytes(const fwi_shot *shots, int nshot, int nz, int nx, int nt, int pml, int problem,
+                                  int filter);
+
+/* ---------------------------------------------------------------- serving
+ * A request loop on one GPU (no counterpart in the reference, which runs one job per process).
+ * Requests of any grid size arrive through fwi_server_submit from any thread; the server admits
+ * the oldest one as soon as one of `max_active` workers is free and its footprint
+ * (fwi_request_bytes) fits into `hbm_budget` (0: 90 % of the free device memory) beside the
+ * requests already running, and runs admitted requests concurrently, each on its own stream.
+ * Results are written into the caller's buffers, which must stay valid until fwi_server_wait
+ * reports the request done.  fwi_server_destroy finishes every submitted request first. */
+typedef struct fwi_server fwi_server;
+enum { FWI_REQ_MODEL = 0, FWI_REQ_GRADIENT = 1 };
+enum { FWI_REQ_QUEUED = 0, FWI_REQ_RUNNING = 1, FWI_REQ_DONE = 2, FWI_REQ_FAILED = 3 };
+typedef struct fwi_request {
+    int kind;                     /* FWI_REQ_MODEL (modeling, problem 0) or FWI_REQ_GRADIENT (problem 1) */
+    int nz, nx;                   /* model grid; vp and rho are [nx][nz] host arrays */
+    float dx, dz, dt;
+    int nt, pml, fs;
+    const float *vp, *rho;
+    const fwi_shot *shots;
+    int nshot;
+    const float *const *obs;      /* gradient: observed traces per shot, [ntr][ns] */
+    float freq;                   /* residual filter frequency (0: the shot's fpeak) */
+    int filter, precondition;     /* as iso_acoustic2d_propagation */
+    float *const *traces;         /* out, per shot [ntr][ns] or NULL: seismograms / adjoint sources */
+    float *grad;                  /* out, gradient [nx][nz] (gradient requests) or NULL */
+} fwi_request;
+typedef struct fwi_request_info {
+    int state, status;            /* FWI_REQ_*; FWI_OK or the engine's error code */
+    size_t bytes;                 /* admitted footprint */
+    double queue_ms, run_ms, total_ms;
+    double objective;             /* misfit of a gradient request */
+    double cell_updates;
+    char error[256];
+} fwi_request_info;
+typedef struct fwi_server_stats {
+    long long submitted, completed, failed, rejected;
+    double p50_ms, p99_ms, max_ms;          /* submission to completion */
+    double p50_queue_ms, p99_queue_ms;      /* submission to admission */
+    double wall_s;                          /* first submission to last completion */
+    double cell_updates, shots_modeled, shot_gradients;
+    size_t budget, peak_bytes;
+    int max_active, peak_active;
+} fwi_server_report;
+FWI_API int fwi_server_create(fwi_server **out, int device, size_t hbm_budget, int max_active);
+FWI_API size_t fwi_request_bytes(const fwi_request *req);
+FWI_API int fwi_server_submit(fwi_server *s, const fwi_request *req, long long *id);
+FWI_API int fwi_server_wait(fwi_server *s, long long id, double timeout_s, fwi_request_info *info);
+FWI_API int fwi_server_stats(fwi_server *s, fwi_server_report *out);
+FWI_API int fwi_server_destroy(fwi_server *s);
+
 /* Shot-sharded runs (one context per GPU, each holding a share of the survey's shots and the
  * whole model).  The path has one exchange step per gradient: the FP64 stacks of the gradient
  * and of the pseudo-Hessian (propagation.c:953-976 stacks them over shots) and the
