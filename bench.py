@@ -305,6 +305,66 @@ class ContextE2E:
         return r
 
 
+# ------------------------------------------------------------------ serving
+SERVE_GRIDS = [(221, 601, 12.5, 0.001), (301, 901, 12.5, 0.001), (401, 1201, 10.0, 0.0008), (601, 2001, 10.0, 0.0008)]
+
+
+def serving(E, M, nreq, rate, seed=0, max_active=4):
+    """The serving loop under a Poisson stream of mixed requests (the serving configuration of the
+    survey: 70 % one-shot modeling, 30 % 8-shot gradients, grids from four sizes, nt uniform in
+    2001..6001), submitted as they arrive; latency from submission to completion."""
+    rng = np.random.default_rng(seed)
+    models = {}
+    for g, (nz, nx, dx, dt) in enumerate(SERVE_GRIDS):
+        vp = M.layered_model(nz, nx, seed=100 + g, water_rows=WATER)
+        models[g] = (vp, M.gardner(vp, water_rows=WATER))
+    plan = []
+    t = 0.0
+    for i in range(nreq):
+        t += rng.exponential(1.0 / rate)
+        g = int(rng.integers(len(SERVE_GRIDS)))
+        nz, nx, dx, dt = SERVE_GRIDS[g]
+        nt = int(rng.integers(2001, 6002))
+        grad = rng.random() < 0.3
+        nshot = 8 if grad else 1
+        src = M.ricker(nt, dt, 10.0, 0.15)
+        first = int(rng.integers(0, nx - 8 * 20))
+        sv = M.line_survey(nz, nx, dx, dx, dt, nt, nshot, src, spacing_cells=20, first_cell=first)
+        shots = M.survey_shots(sv)
+        vp, rho = models[g]
+        kw = dict(vp=vp, rho=rho, dx=dx, dz=dx, dt=dt, nt=nt, pml=PML, fs=FS, shots=shots)
+        if grad:
+            zero = np.zeros((len(shots[0].igx), shots[0].ns), np.float32)  # one host array for all 8 shots
+            kw["obs"] = [zero] * nshot
+        req, holder = E.request(E.REQ_GRADIENT if grad else E.REQ_MODEL, **kw)
+        plan.append((t, req, holder, grad, nshot))
+    srv = E.Server(0, 0, max_active=max_active)
+    ids = []
+    t0 = time.perf_counter()
+    for at, req, holder, _, _ in plan:  # submit at the arrival times
+        dly = at - (time.perf_counter() - t0)
+        if dly > 0:
+            time.sleep(dly)
+        ids.append(srv.submit(req, holder))
+    infos = [srv.wait(i) for i in ids]
+    wall = time.perf_counter() - t0
+    rep = srv.report()
+    srv.close()
+    ok = [x for x in infos if x["status"] == 0]
+    ngrad = sum(p[4] for p in plan if p[3])
+    nmod = sum(p[4] for p in plan if not p[3])
+    return {"requests": nreq, "arrival_rate_per_s": rate, "completed": rep["completed"], "failed": rep["failed"],
+            "mix": "70% 1-shot modeling, 30% 8-shot gradient; grids 221x601@12.5m, 301x901@12.5m, 401x1201@10m, "
+                   "601x2001@10m; nt uniform 2001..6001; Poisson arrivals",
+            "latency_ms": {"p50": rep["p50_ms"], "p99": rep["p99_ms"], "max": rep["max_ms"]},
+            "queue_ms": {"p50": rep["p50_queue_ms"], "p99": rep["p99_queue_ms"]},
+            "service_ms": {"p50": float(np.percentile([x["run_ms"] for x in ok], 50)) if ok else None,
+                           "p99": float(np.percentile([x["run_ms"] for x in ok], 99)) if ok else None},
+            "requests_per_s": len(ok) / wall, "shot_gradients_per_s": ngrad / wall, "shots_modeled_per_s": nmod / wall,
+            "gcells_per_s": rep["cell_updates"] / wall / 1e9, "wall_s": wall, "max_active": rep["max_active"],
+            "peak_active": rep["peak_active"], "peak_admitted_bytes": rep["peak_bytes"], "budget_bytes": rep["budget"]}
+
+
 # ------------------------------------------------------------------ roofline
 TRAFFIC = os.path.join(ROOT, "profiles", "k_tile_forward_60shots_traffic.json")
 
@@ -365,6 +425,8 @@ def main():
     ap.add_argument("--impl", default="mine", choices=["mine", "reference"])
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline sample")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--serve-requests", type=int, default=40, help="requests of the serving measurement (0: skip)")
+    ap.add_argument("--serve-rate", type=float, default=20.0, help="Poisson arrival rate of the serving measurement")
     ap.add_argument("--step-case", nargs=2, type=int, metavar=("SHOTS", "NT"),
                     help="profiling case: one batched forward of SHOTS shots of the survey for NT steps, no JSON line")
     args = ap.parse_args()
@@ -484,6 +546,11 @@ def main():
                "d2h_bytes_per_step": int(d.d2h), "steps": ne,
                "path": "iso_acoustic2d_propagation + smooth2D/objective/perturbation/step-length C-ABI, pinned host"}
 
+    serve = None
+    if args.serve_requests > 0 and not sharded:
+        from fwiedu import models as M
+        serve = serving(E, M, args.serve_requests, args.serve_rate)
+
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
         try:
@@ -512,6 +579,7 @@ def main():
                           "note": "one shot per launch, same iteration minus the host model update, 2 shots"},
                 "batched_over_plain": value / world / plain_sgps,
                 "wall_s": wall, "gpu_launches": launches, "roofline": roof, "cpu_baseline": cpu, "e2e": e2e,
+                "serving": serve,
                 "clocks": clk.summary()}
         print(json.dumps(line), flush=True)
     ctx.close()
