@@ -27,6 +27,7 @@
 #include <cstring>
 #include <cstdint>
 #include <deque>
+#include <tuple>
 #include <map>
 #include <memory>
 #include <mutex>
@@ -137,6 +138,8 @@ struct fwi_ctx {
     fwi_stats stats{};
     int math = 0;  // 0: bit-exact arithmetic, 1: contracted multiply-adds
     bool use_graphs = true;  // capture the batched launch sequences as CUDA graphs
+    bool tune = true;        // time the step kernel's launch shapes once per shape (autotune)
+    int last_tx = 0, last_nst = 0, last_chunk = 0;  // the shape of the last launch
     int *d_err = nullptr;  // set by a step kernel whose tile copy did not complete
     std::map<void *, size_t> sizes;  // live device blocks of this context
     size_t peak = 0;
@@ -223,6 +226,7 @@ extern "C" int fwi_ctx_create(fwi_ctx **out, int device, size_t budget)
     c->budget = budget;
     if (const char *e = getenv("FWI_MATH")) c->math = atoi(e) ? 1 : 0;
     if (const char *e = getenv("FWI_GRAPH")) c->use_graphs = e[0] != '0';  // 0: direct launches (profilers)
+    if (const char *e = getenv("FWI_TUNE")) c->tune = e[0] != '0';            // 0: heuristic launch shapes
     CK(cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking));
     CK(cudaEventCreate(&c->ev0));
     CK(cudaEventCreate(&c->ev1));
@@ -818,6 +822,141 @@ static int pick_chunk(int tiles, int nshot, int resident)
     return 1;
 }
 
+static int check_kernel_error(fwi_ctx *c);
+
+// ---------------------------------------------------------------- tile configuration and autotuner
+// A launch shape of the step kernel: tile width (8 or 16 columns), depth of the shared-memory
+// ring (2..4 shots in flight) and shots per block (the chunk).
+struct TileCfg {
+    int tx = 16, nst = 4, chunk = 1;
+};
+
+static int launch_tiles(fwi_ctx *c, const Program *prog, int L0, int L1, int shot_base, int nshot, const ShotRun *r0,
+                        const TileCfg &cfg)
+{
+    const Plan *p = r0->plan;
+    const int zt = (p->G + TG - 1) / TG;
+    const int tx = cfg.tx, nst = cfg.nst, chunk = cfg.chunk;
+    TileFn fn = tx == 16 ? (c->math ? tile_fn_nst<16, 1>(nst) : tile_fn_nst<16, 0>(nst))
+                         : (c->math ? tile_fn_nst<8, 1>(nst) : tile_fn_nst<8, 0>(nst));
+    const int smem = tx == 16 ? TileGeom<16>::smem(nst) : TileGeom<8>::smem(nst);
+    const int ntx = (p->Nx + tx - 1) / tx, nchunks = (nshot + chunk - 1) / chunk;
+    dim3 grid(ntx + 1, 2 * nchunks, zt);
+    CUtensorMap m1, m0, mc;
+    if (tx == 16) TRY(encode_group_maps<16>(r0->d, nshot, p->d_coef, &m1, &m0, &mc));
+    else TRY(encode_group_maps<8>(r0->d, nshot, p->d_coef, &m1, &m0, &mc));
+    for (int L = L0; L < L1; L++) {
+        const int4 &pw = prog->items[L];
+        if (pw.x == K_NONE && pw.z == K_NONE) continue;
+        fn<<<grid, dim3(TG, tx + 2), smem, c->stream>>>(m1, m0, mc, c->d_desc, prog->d, L, shot_base, nshot, chunk,
+                                                         c->d_err);
+        c->launches++;
+    }
+    CK(cudaGetLastError());
+    return FWI_OK;
+}
+
+// the measured best configuration per launch shape, shared by every context of the process
+struct TuneKey {
+    int Nx, G, nshot, math, batched;
+    bool operator<(const TuneKey &o) const
+    {
+        return std::tie(Nx, G, nshot, math, batched) < std::tie(o.Nx, o.G, o.nshot, o.math, o.batched);
+    }
+};
+static std::mutex g_tune_mu;
+static std::map<TuneKey, TileCfg> g_tune;
+
+// the heuristic shape, or the tuned one, with the environment's overrides applied last
+static TileCfg tile_config(fwi_ctx *c, const Plan *p, int nshot, bool batched)
+{
+    TileCfg cfg;
+    cfg.tx = batched ? 16 : 8;
+    cfg.nst = 4;
+    const int zt = (p->G + TG - 1) / TG;
+    cfg.chunk = pick_chunk(((p->Nx + cfg.tx - 1) / cfg.tx) * zt, nshot, cfg.tx == 16 ? 2 : 4);
+    {
+        std::lock_guard<std::mutex> lk(g_tune_mu);
+        auto it = g_tune.find({p->Nx, p->G, nshot, c->math, batched ? 1 : 0});
+        if (it != g_tune.end()) cfg = it->second;
+    }
+    if (const char *e = getenv("FWI_TX")) cfg.tx = atoi(e) == 8 ? 8 : 16;
+    if (const char *e = getenv("FWI_NST")) cfg.nst = std::min(4, std::max(2, atoi(e)));
+    if (const char *e = getenv("FWI_CHUNK")) cfg.chunk = std::min(TILE_CH_MAX, std::max(1, atoi(e)));
+    cfg.chunk = std::min(cfg.chunk, std::max(1, nshot));
+    c->last_tx = cfg.tx;
+    c->last_nst = cfg.nst;
+    c->last_chunk = cfg.chunk;
+    return cfg;
+}
+
+// Time candidate shapes on this group's own forward scratch frames (forward steps 1..12 of the
+// real shots, three warm-up launches first) and keep the fastest for this launch shape.  The
+// scratch frames are zeroed again afterwards, which is the state a pass starts from; the
+// samples the probe wrote are overwritten by the pass.  Candidates: tile width 8/16, ring
+// depth 2..4, and chunks of at most 4/8/12/16/24 shots (split evenly).
+static int autotune(fwi_ctx *c, int shot_base, int nshot, const ShotRun *r0, bool batched)
+{
+    const Plan *p = r0->plan;
+    const TuneKey key{p->Nx, p->G, nshot, c->math, batched ? 1 : 0};
+    {
+        std::lock_guard<std::mutex> lk(g_tune_mu);
+        if (g_tune.count(key)) return FWI_OK;
+    }
+    const int steps = std::min(12, std::max(2, c->nt - 2));
+    std::vector<int4> items;
+    for (int it = 1; it <= steps; it++) items.push_back(make_int4(K_FWD0, it, K_NONE, 0));
+    Program *prog;
+    TRY(get_program(c, "tune/" + std::to_string(steps), items, &prog));
+    std::vector<TileCfg> cands;
+    for (int tx : {16, 8})
+        for (int nst : {2, 3, 4}) {
+            std::set<int> chunks;
+            for (int cap : {4, 8, 12, 16, 24}) {
+                const int nch = (nshot + cap - 1) / cap;
+                chunks.insert((nshot + nch - 1) / nch);
+            }
+            for (int ch : chunks) {
+                if (nshot == 1 && nst != 2) continue;  // one shot: the ring depth does not matter
+                TileCfg t;
+                t.tx = tx;
+                t.nst = nst;
+                t.chunk = ch;
+                cands.push_back(t);
+            }
+        }
+    const long long l0 = c->launches;
+    float best_ms = 1e30f;
+    TileCfg best;
+    cudaEvent_t e0, e1;  // the context's own events time the whole run
+    CK(cudaEventCreate(&e0));
+    CK(cudaEventCreate(&e1));
+    for (const TileCfg &t : cands) {
+        TRY(launch_tiles(c, prog, 0, std::min(3, steps), shot_base, nshot, r0, t));  // warm-up
+        CK(cudaEventRecord(e0, c->stream));
+        TRY(launch_tiles(c, prog, 0, steps, shot_base, nshot, r0, t));
+        CK(cudaEventRecord(e1, c->stream));
+        CK(cudaEventSynchronize(e1));
+        float ms = 0.f;
+        CK(cudaEventElapsedTime(&ms, e0, e1));
+        if (ms < best_ms) {
+            best_ms = ms;
+            best = t;
+        }
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    c->launches = l0;  // probe launches are not part of the run
+    for (int i = 0; i < nshot; i++) {
+        const ShotRun *r = c->runs.size() == 1 ? c->runs[0].get() : c->runs[shot_base + i].get();
+        CK(cudaMemsetAsync(frame_ptr(r->d, F_FWD), 0, 3 * (size_t)r->d.frame * 4, c->stream));
+    }
+    TRY(check_kernel_error(c));
+    std::lock_guard<std::mutex> lk(g_tune_mu);
+    g_tune[key] = best;
+    return FWI_OK;
+}
+
 static int launch_steps(fwi_ctx *c, const Program *prog, int shot_base, int nshot, const ShotRun *r0, bool batched)
 {
     const Plan *p = r0->plan;
@@ -837,30 +976,8 @@ static int launch_steps(fwi_ctx *c, const Program *prog, int shot_base, int nsho
         CK(cudaGetLastError());
         return FWI_OK;
     }
-    int tx = batched ? 16 : 8;
-    if (const char *e = getenv("FWI_TX")) tx = atoi(e) == 8 ? 8 : 16;
-    int nst = 4;
-    if (const char *e = getenv("FWI_NST")) nst = std::min(4, std::max(2, atoi(e)));
-    const int ntx = (p->Nx + tx - 1) / tx;
-    int chunk = pick_chunk(ntx * zt, nshot, tx == 16 ? 2 : 4);
-    if (const char *e = getenv("FWI_CHUNK")) chunk = std::min(TILE_CH_MAX, std::max(1, atoi(e)));
-    TileFn fn = tx == 16 ? (c->math ? tile_fn_nst<16, 1>(nst) : tile_fn_nst<16, 0>(nst))
-                         : (c->math ? tile_fn_nst<8, 1>(nst) : tile_fn_nst<8, 0>(nst));
-    const int smem = tx == 16 ? TileGeom<16>::smem(nst) : TileGeom<8>::smem(nst);
-    const int nchunks = (nshot + chunk - 1) / chunk;
-    dim3 grid(ntx + 1, 2 * nchunks, zt);
-    CUtensorMap m1, m0, mc;
-    if (tx == 16) TRY(encode_group_maps<16>(r0->d, nshot, p->d_coef, &m1, &m0, &mc));
-    else TRY(encode_group_maps<8>(r0->d, nshot, p->d_coef, &m1, &m0, &mc));
-    for (int L = 0; L < n; L++) {
-        const int4 &pw = prog->items[L];
-        if (pw.x == K_NONE && pw.z == K_NONE) continue;
-        fn<<<grid, dim3(TG, tx + 2), smem, c->stream>>>(m1, m0, mc, c->d_desc, prog->d, L, shot_base, nshot, chunk,
-                                                         c->d_err);
-        c->launches++;
-    }
-    CK(cudaGetLastError());
-    return FWI_OK;
+    const TileCfg cfg = tile_config(c, p, nshot, batched);
+    return launch_tiles(c, prog, 0, n, shot_base, nshot, r0, cfg);
 }
 
 // a step kernel that gave up waiting for a tile copy leaves its mark in the error word
@@ -1272,6 +1389,10 @@ static int adj_init(fwi_ctx *c, const std::vector<ShotRun *> &rs, int shot_base)
 static int run_program(fwi_ctx *c, const std::string &key, const Program *prog, int shot_base, int nshot,
                        const ShotRun *r0, bool batched)
 {
+    const char *ke = getenv("FWI_KERNEL");
+    const bool tile_kernel = !(ke && strcmp(ke, "step") == 0);
+    if (c->tune && tile_kernel && !getenv("FWI_TX") && !getenv("FWI_NST") && !getenv("FWI_CHUNK"))
+        TRY(autotune(c, shot_base, nshot, r0, batched));
     if (!batched) return launch_steps(c, prog, shot_base, nshot, r0, false);
     if (!c->use_graphs) return launch_steps(c, prog, shot_base, nshot, r0, true);
     auto it = c->graphs.find(key);
@@ -1507,6 +1628,22 @@ extern "C" int fwi_ctx_objective(fwi_ctx *c, double *out)
     }
     TRY(exchange_scalars(c, &acc, 1));
     *out = 0.5 * acc;
+    return FWI_OK;
+}
+
+extern "C" int fwi_ctx_set_autotune(fwi_ctx *c, int on)
+{
+    if (!c) return fail(FWI_ERR_ARG, "ctx is NULL");
+    c->tune = on != 0;
+    return FWI_OK;
+}
+
+extern "C" int fwi_ctx_launch_shape(fwi_ctx *c, int *tile_columns, int *ring_depth, int *shots_per_block)
+{
+    if (!c) return fail(FWI_ERR_ARG, "ctx is NULL");
+    if (tile_columns) *tile_columns = c->last_tx;
+    if (ring_depth) *ring_depth = c->last_nst;
+    if (shots_per_block) *shots_per_block = c->last_chunk;
     return FWI_OK;
 }
 

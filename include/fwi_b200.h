@@ -188,6 +188,14 @@ typedef struct {
 } fwi_stats;
 FWI_API int fwi_ctx_stats(fwi_ctx *ctx, fwi_stats *out);
 
+/* The step kernel's launch shape (tile width 8/16 columns, shared-memory ring depth 2..4 shots,
+ * shots per block) is picked by an autotuner: the first run of a launch shape (padded grid,
+ * shots per launch, arithmetic, path) times the candidates on the run's own scratch frames and
+ * keeps the fastest for the process.  Off (or FWI_TUNE=0; or FWI_TX / FWI_NST / FWI_CHUNK set):
+ * a built-in heuristic.  fwi_ctx_launch_shape reports the shape of the last launch. */
+FWI_API int fwi_ctx_set_autotune(fwi_ctx *ctx, int on);
+FWI_API int fwi_ctx_launch_shape(fwi_ctx *ctx, int *tile_columns, int *ring_depth, int *shots_per_block);
+
 /* CUDA graphs on the batched path (default on; FWI_GRAPH=0 in the environment turns them off):
  * off, every step is launched directly -- cheaper for a launch sequence run only once. */
 FWI_API int fwi_ctx_set_graphs(fwi_ctx *ctx, int on);

@@ -26,7 +26,7 @@ SHAPES = [
     {"FWI_TX": "16", "FWI_NST": "4", "FWI_CHUNK": "2"},
     {"FWI_TX": "16", "FWI_NST": "3", "FWI_CHUNK": "32"},
 ]
-KEYS = ("FWI_TX", "FWI_NST", "FWI_CHUNK", "FWI_KERNEL", "FWI_MATH")
+KEYS = ("FWI_TX", "FWI_NST", "FWI_CHUNK", "FWI_KERNEL", "FWI_MATH", "FWI_TUNE")
 
 
 def rel(a, b):
@@ -128,3 +128,28 @@ def test_contracted_math_within_tolerance():
         assert rel(pre[i], c.obs[i]) <= 1e-5
         assert rel(adj[i], c.adj[i]) <= 1e-4
     assert rel(grad, c.grad) <= 1e-4
+
+
+def test_autotuned_shape_is_bit_identical_and_cached():
+    """The autotuner times launch shapes on the run's own scratch frames: the run it precedes
+    must give the same bits as with the heuristic shape, and the shape is kept for the process."""
+    c = Case("fs1_small")
+    with env(FWI_TUNE="0"):
+        ref_pre, _ = run_case(c.vp, c.rho, c.dx, c.dt, c.nt, c.pml, c.fs, c.shots)
+        ref_adj, ref_grad = run_case(c.vp0, c.rho0, c.dx, c.dt, c.nt, c.pml, c.fs, c.shots, obs=c.obs)
+    with env():
+        pre, _ = run_case(c.vp, c.rho, c.dx, c.dt, c.nt, c.pml, c.fs, c.shots)
+        adj, grad = run_case(c.vp0, c.rho0, c.dx, c.dt, c.nt, c.pml, c.fs, c.shots, obs=c.obs)
+        ctx = E.Context(0)
+        ctx.set_model(c.vp, c.rho, c.dx, c.dx, c.dt, c.nt, c.pml, c.fs)
+        ctx.set_shots(c.shots)
+        ctx.run(0, path=E.PATH_BATCHED)
+        L = E.lib()
+        import ctypes as C
+        tx, nst, ch = C.c_int(), C.c_int(), C.c_int()
+        L.fwi_ctx_launch_shape(ctx.h, C.byref(tx), C.byref(nst), C.byref(ch))
+        ctx.close()
+    assert tx.value in (8, 16) and 2 <= nst.value <= 4 and 1 <= ch.value <= c.nshot
+    assert all(np.array_equal(a, b) for a, b in zip(pre, ref_pre))
+    assert all(np.array_equal(a, b) for a, b in zip(adj, ref_adj))
+    assert np.array_equal(grad, ref_grad)
