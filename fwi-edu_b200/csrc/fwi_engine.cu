@@ -139,7 +139,7 @@ struct fwi_ctx {
     int math = 0;  // 0: bit-exact arithmetic, 1: contracted multiply-adds
     bool use_graphs = true;  // capture the batched launch sequences as CUDA graphs
     bool tune = true;        // time the step kernel's launch shapes once per shape (autotune)
-    int last_tx = 0, last_nst = 0, last_chunk = 0;  // the shape of the last launch
+    int last_tx = 0, last_nst = 0, last_chunk = 0, last_gpt = 0;  // the shape of the last launch
     int *d_err = nullptr;  // set by a step kernel whose tile copy did not complete
     std::map<void *, size_t> sizes;  // live device blocks of this context
     size_t peak = 0;
@@ -782,11 +782,11 @@ static LaunchCfg pick_launch(int Nx, int nshot, bool batched, int math)
 typedef void (*TileFn)(const CUtensorMap, const CUtensorMap, const CUtensorMap, const ShotDesc *, const int4 *, int,
                        int, int, int, int *);
 
-template <int TX, int NST, int MATH>
+template <int TX, int NST, int MATH, int GPT>
 static TileFn tile_fn()
 {
     static bool ready = false;
-    TileFn f = k_tile<TX, NST, MATH>;
+    TileFn f = k_tile<TX, NST, MATH, GPT>;
     if (!ready) {
         cudaFuncSetAttribute((const void *)f, cudaFuncAttributeMaxDynamicSharedMemorySize, TileGeom<TX>::smem(NST));
         cudaFuncSetAttribute((const void *)f, cudaFuncAttributePreferredSharedMemoryCarveout,
@@ -796,10 +796,16 @@ static TileFn tile_fn()
     return f;
 }
 
-template <int TX, int MATH>
+template <int TX, int MATH, int GPT>
 static TileFn tile_fn_nst(int nst)
 {
-    return nst == 2 ? tile_fn<TX, 2, MATH>() : nst == 4 ? tile_fn<TX, 4, MATH>() : tile_fn<TX, 3, MATH>();
+    return nst == 2 ? tile_fn<TX, 2, MATH, GPT>() : nst == 4 ? tile_fn<TX, 4, MATH, GPT>() : tile_fn<TX, 3, MATH, GPT>();
+}
+
+template <int TX, int MATH>
+static TileFn tile_fn_gpt(int nst, int gpt)
+{
+    return gpt == 2 ? tile_fn_nst<TX, MATH, 2>(nst) : tile_fn_nst<TX, MATH, 1>(nst);
 }
 
 // shots per block: split the group into equal chunks (at most 12 shots each, the measured
@@ -828,7 +834,7 @@ static int check_kernel_error(fwi_ctx *c);
 // A launch shape of the step kernel: tile width (8 or 16 columns), depth of the shared-memory
 // ring (2..4 shots in flight) and shots per block (the chunk).
 struct TileCfg {
-    int tx = 16, nst = 4, chunk = 1;
+    int tx = 16, nst = 4, chunk = 1, gpt = 1;  // gpt: z-groups per consumer thread (1 or 2)
 };
 
 static int launch_tiles(fwi_ctx *c, const Program *prog, int L0, int L1, int shot_base, int nshot, const ShotRun *r0,
@@ -836,9 +842,9 @@ static int launch_tiles(fwi_ctx *c, const Program *prog, int L0, int L1, int sho
 {
     const Plan *p = r0->plan;
     const int zt = (p->G + TG - 1) / TG;
-    const int tx = cfg.tx, nst = cfg.nst, chunk = cfg.chunk;
-    TileFn fn = tx == 16 ? (c->math ? tile_fn_nst<16, 1>(nst) : tile_fn_nst<16, 0>(nst))
-                         : (c->math ? tile_fn_nst<8, 1>(nst) : tile_fn_nst<8, 0>(nst));
+    const int tx = cfg.tx, nst = cfg.nst, chunk = cfg.chunk, gpt = cfg.gpt, nl = TG / gpt;
+    TileFn fn = tx == 16 ? (c->math ? tile_fn_gpt<16, 1>(nst, gpt) : tile_fn_gpt<16, 0>(nst, gpt))
+                         : (c->math ? tile_fn_gpt<8, 1>(nst, gpt) : tile_fn_gpt<8, 0>(nst, gpt));
     const int smem = tx == 16 ? TileGeom<16>::smem(nst) : TileGeom<8>::smem(nst);
     const int ntx = (p->Nx + tx - 1) / tx, nchunks = (nshot + chunk - 1) / chunk;
     dim3 grid(ntx + 1, 2 * nchunks, zt);
@@ -848,8 +854,8 @@ static int launch_tiles(fwi_ctx *c, const Program *prog, int L0, int L1, int sho
     for (int L = L0; L < L1; L++) {
         const int4 &pw = prog->items[L];
         if (pw.x == K_NONE && pw.z == K_NONE) continue;
-        fn<<<grid, dim3(TG, tx + 2), smem, c->stream>>>(m1, m0, mc, c->d_desc, prog->d, L, shot_base, nshot, chunk,
-                                                         c->d_err);
+        fn<<<grid, dim3(nl, tx + 32 / nl), smem, c->stream>>>(m1, m0, mc, c->d_desc, prog->d, L, shot_base, nshot,
+                                                               chunk, c->d_err);
         c->launches++;
     }
     CK(cudaGetLastError());
@@ -883,10 +889,12 @@ static TileCfg tile_config(fwi_ctx *c, const Plan *p, int nshot, bool batched)
     if (const char *e = getenv("FWI_TX")) cfg.tx = atoi(e) == 8 ? 8 : 16;
     if (const char *e = getenv("FWI_NST")) cfg.nst = std::min(4, std::max(2, atoi(e)));
     if (const char *e = getenv("FWI_CHUNK")) cfg.chunk = std::min(TILE_CH_MAX, std::max(1, atoi(e)));
+    if (const char *e = getenv("FWI_GPT")) cfg.gpt = atoi(e) == 2 ? 2 : 1;
     cfg.chunk = std::min(cfg.chunk, std::max(1, nshot));
     c->last_tx = cfg.tx;
     c->last_nst = cfg.nst;
     c->last_chunk = cfg.chunk;
+    c->last_gpt = cfg.gpt;
     return cfg;
 }
 
@@ -909,22 +917,24 @@ static int autotune(fwi_ctx *c, int shot_base, int nshot, const ShotRun *r0, boo
     Program *prog;
     TRY(get_program(c, "tune/" + std::to_string(steps), items, &prog));
     std::vector<TileCfg> cands;
-    for (int tx : {16, 8})
-        for (int nst : {2, 3, 4}) {
-            std::set<int> chunks;
-            for (int cap : {4, 8, 12, 16, 24}) {
-                const int nch = (nshot + cap - 1) / cap;
-                chunks.insert((nshot + nch - 1) / nch);
+    for (int gpt : {1, 2})
+        for (int tx : {16, 8})
+            for (int nst : {2, 3, 4}) {
+                std::set<int> chunks;
+                for (int cap : {4, 8, 12, 16, 24}) {
+                    const int nch = (nshot + cap - 1) / cap;
+                    chunks.insert((nshot + nch - 1) / nch);
+                }
+                for (int ch : chunks) {
+                    if (nshot == 1 && nst != 2) continue;  // one shot: the ring depth does not matter
+                    TileCfg t;
+                    t.tx = tx;
+                    t.nst = nst;
+                    t.chunk = ch;
+                    t.gpt = gpt;
+                    cands.push_back(t);
+                }
             }
-            for (int ch : chunks) {
-                if (nshot == 1 && nst != 2) continue;  // one shot: the ring depth does not matter
-                TileCfg t;
-                t.tx = tx;
-                t.nst = nst;
-                t.chunk = ch;
-                cands.push_back(t);
-            }
-        }
     const long long l0 = c->launches;
     float best_ms = 1e30f;
     TileCfg best;
@@ -1391,7 +1401,7 @@ static int run_program(fwi_ctx *c, const std::string &key, const Program *prog, 
 {
     const char *ke = getenv("FWI_KERNEL");
     const bool tile_kernel = !(ke && strcmp(ke, "step") == 0);
-    if (c->tune && tile_kernel && !getenv("FWI_TX") && !getenv("FWI_NST") && !getenv("FWI_CHUNK"))
+    if (c->tune && tile_kernel && !getenv("FWI_TX") && !getenv("FWI_NST") && !getenv("FWI_CHUNK") && !getenv("FWI_GPT"))
         TRY(autotune(c, shot_base, nshot, r0, batched));
     if (!batched) return launch_steps(c, prog, shot_base, nshot, r0, false);
     if (!c->use_graphs) return launch_steps(c, prog, shot_base, nshot, r0, true);

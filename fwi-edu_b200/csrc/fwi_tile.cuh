@@ -226,20 +226,23 @@ struct TileGeom {
     static constexpr int smem(int nst) { return ST_OFF + nst * STAGE; }
 };
 // grid: x = column tile (plus one receiver-sampling index), y = 2 * shot chunk + program
-// item, z = tile of TG z-groups.  block = TG x (TX + 2) threads: rows 0..TX-1 are the
-// consumers (one z-group of one column each), the last two rows form the producer warp.
+// item, z = tile of TG z-groups.  block = (TG / GPT) x (TX + 32 / (TG / GPT)) threads: rows
+// 0..TX-1 are the consumers (GPT consecutive z-groups of one column each), the remaining rows
+// form the producer warp.
 // Dynamic shared memory: TileGeom<TX>::smem(NST).
 // Tensor maps: tm_p1 / tm_p0 describe the group's frame pool {ld, Nx, nfr, nshot} (z
 // contiguous; shot s of the group at index s - shot_base) with boxes {ZP, XP, 1, 1} and
 // {ZC, TX, 1, 1}; tm_cf the six coefficient planes {ld, Nx, 6} with box {ZC, TX, 6}.
-template <int TX, int NST, int MATH>
-__global__ void __launch_bounds__(TG *(TX + 2))
+template <int TX, int NST, int MATH, int GPT>
+__global__ void __launch_bounds__(TG / GPT * TX + 32)
     k_tile(const __grid_constant__ CUtensorMap tm_p1, const __grid_constant__ CUtensorMap tm_p0,
            const __grid_constant__ CUtensorMap tm_cf, const ShotDesc *__restrict__ shots, const int4 *__restrict__ prog,
            int L, int shot_base, int nshot, int chunk, int *err)
 {
     using Geo = TileGeom<TX>;
-    constexpr int NT = TG * (TX + 2), NW = TG * TX / 32;
+    constexpr int NL = TG / GPT;  // consumer lanes per column
+    constexpr int NT = NL * TX + 32, NW = NL * TX / 32;
+    static_assert(NL * TX >= 32 && 32 % NL == 0, "whole consumer warps, at least one");
     extern __shared__ __align__(128) unsigned char smem[];
     __shared__ __align__(8) unsigned long long full[NST], empty[NST], cfbar;
     __shared__ float *s_out[TILE_CH_MAX];
@@ -261,7 +264,7 @@ __global__ void __launch_bounds__(TG *(TX + 2))
     const int Nx = A.Nx, pml = A.pml, G = A.G, Nz = A.Nz;
     const int ntx = (Nx + TX - 1) / TX;
     const bool fwd = kind == K_FWD0 || kind == K_FWD1;
-    const int tid = threadIdx.y * TG + threadIdx.x;
+    const int tid = threadIdx.y * NL + threadIdx.x;
     const int warp = tid >> 5, lane = tid & 31;
 
     // ---- the receiver-sampling block: p1 is read-only during this launch
@@ -350,29 +353,24 @@ __global__ void __launch_bounds__(TG *(TX + 2))
         return;
     }
 
-    // ---- per-thread constants
-    const int g = G0 + threadIdx.x, k = threadIdx.y;
-    const int x = X0 + k, z0 = 4 * g;
-    const bool mine = g < G && x < Nx;
+    // ---- consumers: lane zl of column k owns the GPT z-groups G0 + GPT*zl .. G0 + GPT*zl + GPT-1
+    const int zl = threadIdx.x, k = threadIdx.y;
+    const int x = X0 + k;
+    const bool xin = x < Nx, xint = x >= 3 && x <= Nx - 4;
     const int zlo = A.izStart, zhi = Nz - 4;
-    const bool zfd = z0 + 3 >= zlo && z0 <= zhi;
-    const bool zpart = z0 < zlo || z0 + 3 > zhi;  // group straddles the edge of the updated rows
-    const bool any = mine && zfd && x >= 3 && x <= Nx - 4;
     // Free surface.  The reference sets row pml to -0 and mirrors rows pml+1..2pml into rows
     // pml-1..0 (propagation.c:76-101).  Only the three mirrored rows next to the surface are ever
     // read again (the stencil updates rows >= pml and reaches three rows up; receivers, imaging
     // and the Hessian lie at rows >= pml), so only rows pml+1..pml+3 are mirrored here: every
     // seismogram and gradient is the reference's, and the rows above pml-3 are never written.
     const int fs_hi = min(2 * pml, pml + 3);  // last mirrored source row
-    const bool fs_top = A.fs && mine && z0 <= fs_hi;  // the surface row, the mirror source rows, or above
-    const int jpml = (pml >= z0 && pml < z0 + 4) ? pml - z0 : -1;
     const bool inject = kind == K_ADJ && it >= 1;
     const bool hess = kind == K_FWD1 && A.hessian && (it % MST == 0);
     const bool image = kind == K_ADJ && (it % MST == 0);
-    const bool acc_here = mine && (hess || image) && z0 + 3 >= pml && z0 < pml + A.nz && x >= pml && x < pml + A.nxx;
+    const bool xacc = x >= pml && x < pml + A.nxx;
     const bool fs_tile = A.fs && 4 * G0 <= fs_hi;  // tile holds the surface, mirror or rows above
     const bool acc_tile = hess || image;
-    const long long colx = (long long)x * A.ld, col = colx + z0;
+    const long long colx = (long long)x * A.ld;
     const float invdx = A.invdx, invdz = A.invdz, invdtdt = A.invdtdt;
     PkConst K;
     K.C1 = pk(0.77793115f, 0.77793115f);
@@ -389,33 +387,43 @@ __global__ void __launch_bounds__(TG *(TX + 2))
     K.nz = pk(A.negzero, A.negzero);
     const float4 zero4 = make_float4(0.f, 0.f, 0.f, 0.f);
     const float4(*scf)[TX][TG] = reinterpret_cast<const float4(*)[TX][TG]>(smem);
-    float4 cf[6];
+    float4 cfh[6];  // one group per thread: its coefficients stay in registers for the chunk
 
-    // one shot of the chunk from ring stage st: stencil, fused epilogue, store
-    auto consume_shot = [&](int i, int st) {
-        const unsigned char *stg = st_base + st * Geo::STAGE;
-        const float4(*sp1)[TG + 2] = reinterpret_cast<const float4(*)[TG + 2]>(stg);
-        const float4(*sp0)[TG] = reinterpret_cast<const float4(*)[TG]>(stg + Geo::P0_OFF);
-        const int cx = k + 3, cg = threadIdx.x + 1;
-        const float4 cq = sp1[cx][cg];
-        const float4 p0 = sp0[k][threadIdx.x];
+    // group gl of the tile for shot i: stencil from the stage, fused epilogue, store;
+    // lo / cq / hi are groups gl-1, gl, gl+1 of column x
+    auto consume_group = [&](int i, const float4 (*sp1)[TG + 2], const float4 (*sp0)[TG], int gl, const float4 &lo,
+                             const float4 &cq, const float4 &hi) {
+        const int g = G0 + gl, z0 = 4 * g;
+        if (g >= G || !xin) return;
+        const int cx = k + 3, cg = gl + 1;
+        const bool zfd = z0 + 3 >= zlo && z0 <= zhi;
+        const float4 p0 = sp0[k][gl];
         float4 v = zero4;
-        if (any) {
+        if (zfd && xint) {
             const float4 xn[6] = {sp1[cx - 3][cg], sp1[cx - 2][cg], sp1[cx - 1][cg],
                                   sp1[cx + 1][cg], sp1[cx + 2][cg], sp1[cx + 3][cg]};
-            v = group2<MATH>(sp1[cx][cg - 1], cq, sp1[cx][cg + 1], xn, cf, p0, K);
-            if (zpart) {
+            if (GPT == 1) {
+                v = group2<MATH>(lo, cq, hi, xn, cfh, p0, K);
+            } else {
+                const float4 cf[6] = {scf[0][k][gl], scf[1][k][gl], scf[2][k][gl],
+                                      scf[3][k][gl], scf[4][k][gl], scf[5][k][gl]};
+                v = group2<MATH>(lo, cq, hi, xn, cf, p0, K);
+            }
+            if (z0 < zlo || z0 + 3 > zhi) {  // group straddles the edge of the updated rows
                 if (z0 < zlo || z0 > zhi) v.x = 0.f;
                 if (z0 + 1 < zlo || z0 + 1 > zhi) v.y = 0.f;
                 if (z0 + 2 < zlo || z0 + 2 > zhi) v.z = 0.f;
                 if (z0 + 3 < zlo || z0 + 3 > zhi) v.w = 0.f;
             }
         }
+        const long long col = colx + z0;
         // most tiles need none of the rare parts of the epilogue: decided per tile and shot
         if (!(fs_tile || acc_tile || s_spec[i])) {
             *reinterpret_cast<float4 *>(s_out[i] + col) = v;
             return;
         }
+        const bool fs_top = A.fs && z0 <= fs_hi;  // the surface row, the mirror source rows, or above
+        const int jpml = (pml >= z0 && pml < z0 + 4) ? pml - z0 : -1;
         const int isx = s_isx[i], isz = s_isz[i];
         const bool src_here = x == isx && isz >= z0 && isz < z0 + 4;
         // forward: the source enters before the free surface, in double (propagation.c:558-564)
@@ -427,7 +435,7 @@ __global__ void __launch_bounds__(TG *(TX + 2))
         }
         // replay: free surface first, then the float source (propagation.c:656-662)
         if (kind == K_REP && src_here) setc(v, isz - z0, fa(comp(v, isz - z0), s_srcf[i]));
-        if (acc_here) {
+        if (acc_tile && xacc && z0 + 3 >= pml && z0 < pml + A.nz) {
             const ShotDesc &D = shots[cb + i];
             const float4 uu = image ? ldg4(s_u[i] + col) : zero4;
             double2 *acc = reinterpret_cast<double2 *>((image ? D.Gacc : D.H) + col);
@@ -473,14 +481,29 @@ __global__ void __launch_bounds__(TG *(TX + 2))
         }
     };
 
+    // one shot of the chunk from ring stage st: the lane's GPT groups, sharing their z-window
+    auto consume_shot = [&](int i, int st) {
+        const unsigned char *stg = st_base + st * Geo::STAGE;
+        const float4(*sp1)[TG + 2] = reinterpret_cast<const float4(*)[TG + 2]>(stg);
+        const float4(*sp0)[TG] = reinterpret_cast<const float4(*)[TG]>(stg + Geo::P0_OFF);
+        const int gl0 = GPT * zl;
+        float4 w[GPT + 2];  // groups gl0-1 .. gl0+GPT of column x (stage rows gl0 .. gl0+GPT+1)
+#pragma unroll
+        for (int q = 0; q < GPT + 2; ++q) w[q] = sp1[k + 3][gl0 + q];
+#pragma unroll
+        for (int j = 0; j < GPT; ++j) consume_group(i, sp1, sp0, gl0 + j, w[j], w[j + 1], w[j + 2]);
+    };
+
     {  // coefficient tiles, once for all shots
         bool ok = mbar_wait(smem_u32(&cfbar), 0);
         if (!__all_sync(0xffffffffu, ok)) {
             if (lane == 0) atomicExch(err, 1);
             return;
         }
+        if (GPT == 1) {
 #pragma unroll
-        for (int f = 0; f < 6; ++f) cf[f] = scf[f][k][threadIdx.x];
+            for (int f = 0; f < 6; ++f) cfh[f] = scf[f][k][zl];
+        }
     }
     for (int i = 0; i < n; ++i) {
         const int st = i % NST;
@@ -489,7 +512,7 @@ __global__ void __launch_bounds__(TG *(TX + 2))
             if (lane == 0) atomicExch(err, 1);
             break;
         }
-        if (mine) consume_shot(i, st);
+        consume_shot(i, st);
         __syncwarp();
         if (lane == 0) mbar_arrive(smem_u32(&empty[st]));
     }

@@ -25,8 +25,11 @@ SHAPES = [
     {"FWI_TX": "8", "FWI_NST": "2", "FWI_CHUNK": "3"},
     {"FWI_TX": "16", "FWI_NST": "4", "FWI_CHUNK": "2"},
     {"FWI_TX": "16", "FWI_NST": "3", "FWI_CHUNK": "32"},
+    {"FWI_GPT": "2"},
+    {"FWI_TX": "8", "FWI_GPT": "2", "FWI_NST": "3", "FWI_CHUNK": "5"},
+    {"FWI_TX": "16", "FWI_GPT": "2", "FWI_NST": "2", "FWI_CHUNK": "1"},
 ]
-KEYS = ("FWI_TX", "FWI_NST", "FWI_CHUNK", "FWI_KERNEL", "FWI_MATH", "FWI_TUNE")
+KEYS = ("FWI_TX", "FWI_NST", "FWI_CHUNK", "FWI_KERNEL", "FWI_MATH", "FWI_TUNE", "FWI_GPT")
 
 
 def rel(a, b):
