@@ -318,6 +318,36 @@ typedef struct {
 
 static int ck_is_stored(int t, int nt, int d) { return t % d == 0 || ((t + 1) % d == 0 && t + 1 < nt); }
 
+/* Precision study of the checkpoint snapshots: 0 keeps them in the oracle's precision; 1 stores
+ * each snapshot as FP16 with its own max-abs scale (the largest magnitude maps to 2^15); 2 as
+ * BF16 (round to nearest even on the top 16 bits of the FP32 pattern).  The replay starts from,
+ * and the imaging reads, the values as they come back. */
+static int g_ck_precision = 0;
+void orc_set_checkpoint_precision(int mode) { g_ck_precision = mode; }
+
+static float bf16_round(float v)
+{
+    uint32_t b;
+    memcpy(&b, &v, 4);
+    b = (b + 0x7fffu + ((b >> 16) & 1u)) & 0xffff0000u;
+    memcpy(&v, &b, 4);
+    return v;
+}
+
+static void quantize_snapshot(real *u, size_t n)
+{
+    if (g_ck_precision == 0) return;
+    double amax = 0.0;
+    for (size_t i = 0; i < n; i++) amax = fmax(amax, fabs((double)u[i]));
+    if (amax == 0.0) return;
+    if (g_ck_precision == 1) {
+        const double to = 32768.0 / amax, back = amax / 32768.0;
+        for (size_t i = 0; i < n; i++) u[i] = (real)((double)(_Float16)((double)u[i] * to) * back);
+    } else {
+        for (size_t i = 0; i < n; i++) u[i] = (real)bf16_round((float)u[i]);
+    }
+}
+
 static void ck_alloc(Ckpt *ck, int nt, size_t frame)
 {
     ck->nt = nt;
@@ -351,8 +381,12 @@ static void engine_forward(const Grid *g, const OrcShot *s, int nt, int mode, in
     if (H) memset(H, 0, sizeof(double) * g->nz * g->nxx);
     for (int it = 0; it < nt; ++it) {
         if (mode == 1 && it % ck->d == 0) {
-            if (it - 1 >= 0) memcpy(ck->store + (size_t)ck->slot[it - 1] * n, p0, frame_bytes(g));
+            if (it - 1 >= 0) {
+                memcpy(ck->store + (size_t)ck->slot[it - 1] * n, p0, frame_bytes(g));
+                quantize_snapshot(ck->store + (size_t)ck->slot[it - 1] * n, n);
+            }
             memcpy(ck->store + (size_t)ck->slot[it] * n, p1, frame_bytes(g));
+            quantize_snapshot(ck->store + (size_t)ck->slot[it] * n, n);
         }
         fd_step(p2, p1, p0, g);
         /* source: the product is formed in double (the literal 1.0), propagation.c:558 */

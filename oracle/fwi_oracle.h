@@ -72,6 +72,8 @@ void orc_taper_traces(float *tr, int nt, int ntr, int taperLenTime, int taperLen
 void orc_adjoint_source(const OrcShot *shot, const float *vp_global, int nz, float freq, int filter,
                         const float *pre, const float *obs, float *adj);
 void orc_shot_precondition(float *grad, float *precond, int n);
+/* checkpoint snapshots stored as 0: oracle precision, 1: FP16 with max-abs scaling, 2: BF16 */
+void orc_set_checkpoint_precision(int mode);
 void orc_global_precondition(float *grad, const float *precond, int n, float alpha);
 /* model update of acoustic2d_fwi.c:425-465 after the step length is known */
 void orc_vp2density(const float *vp, float *rho, int n);

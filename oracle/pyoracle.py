@@ -136,6 +136,10 @@ class Port:
             raise ValueError(f"orc_shot_gradient: status {rc}")
         return pre, g, h
 
+    def set_checkpoint_precision(self, mode):
+        """Checkpoint snapshots: 0 oracle precision, 1 FP16 with max-abs scaling, 2 BF16."""
+        self.lib.orc_set_checkpoint_precision(int(mode))
+
     def global_precondition(self, grad, precond, alpha=0.005):
         """orc_global_precondition on float32 arrays, in place."""
         n = grad.size

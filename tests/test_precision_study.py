@@ -1,0 +1,32 @@
+"""Precision study of the checkpoint snapshots (the replay restarts from them and the imaging
+reads them): may they be stored in FP16 or BF16 with per-snapshot max-abs scaling?  Only if the
+gradient stays within its 1e-4 tolerance.  Measured with the oracle against its FP64 build on
+three golden cases: FP32 snapshots 4e-6..3e-5, FP16 with max-abs scaling 4e-4..5e-4, BF16
+4e-3..5e-3 -- both reduced formats exceed the tolerance, so the engine keeps FP32 snapshots.
+"""
+import numpy as np
+import pytest
+
+from golden_cases import Case
+
+
+def rel(a, b):
+    return float(np.linalg.norm(np.asarray(a, np.float64) - b) / np.linalg.norm(b))
+
+
+@pytest.mark.parametrize("name", ["fs1_small", "noprec", "fs0_small"])
+def test_reduced_precision_snapshots_exceed_the_gradient_tolerance(port32, port64, name):
+    c = Case(name)
+    args = (c.vp0, c.rho0, c.shots, c.dx, c.dx, c.dt, c.nt, c.pml, c.fs, 10.0, 2.0, c.precondition, 1)
+    _, g64 = port64.propagation(*args, obs=c.obs)
+    err = {}
+    try:
+        for mode, label in ((0, "fp32"), (1, "fp16"), (2, "bf16")):
+            port32.set_checkpoint_precision(mode)
+            _, g = port32.propagation(*args, obs=c.obs)
+            err[label] = rel(g, g64)
+    finally:
+        port32.set_checkpoint_precision(0)
+    assert err["fp32"] < 1e-4  # what the engine stores
+    assert 1e-4 < err["fp16"] < 2e-3  # FP16 (max-abs scaled): about its 2^-11 precision, above tolerance
+    assert 1e-3 < err["bf16"] < 2e-2  # BF16: about its 2^-8 precision
