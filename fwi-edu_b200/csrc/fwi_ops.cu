@@ -388,6 +388,123 @@ extern "C" void interpolate_traces(float **tr, int ntr, int nt, int r, float **t
     report(cudaStreamSynchronize(g_ops.st), "interpolate_traces");
 }
 
+// ---- 2-D wavenumber filters: Y = crop(IDFT2(W . DFT2(pad(X)))) / (Nz Nx) as five FP32 GEMMs
+namespace {
+
+void build_wn_window(float *h, const int *ip, const float *fp)
+{
+    fwi_wavenumber_window(ip[0], ip[1], ip[2], fp[0], fp[1], fp[2], fp[3], h);
+}
+void build_wn_fz(float *h, const int *ip, const float *) { fwi_wn_forward_z(ip[0], ip[1], h); }
+void build_wn_fx(float *h, const int *ip, const float *) { fwi_wn_forward_x(ip[0], ip[1], h); }
+void build_wn_ix(float *h, const int *ip, const float *) { fwi_wn_inverse_x(ip[0], ip[1], h); }
+void build_wn_iz(float *h, const int *ip, const float *) { fwi_wn_inverse_z(ip[0], ip[1], h); }
+
+// F[c][r] *= W[c mod Nx][r] over the two Nz x Nx halves (real, imaginary) of the spectrum
+__global__ void k_window2(float *__restrict__ F, const float *__restrict__ W, long long plane)
+{
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < 2 * plane;
+         i += (long long)gridDim.x * blockDim.x)
+        F[i] *= W[i < plane ? i : i - plane];
+}
+
+void wavenumber_filter(float **s, int nz, int nx, float dz, float dx, float kpass, float kcut, float **s_filter,
+                       int filter, const char *name)
+{
+    std::lock_guard<std::mutex> lk(g_ops_mu);
+    if (!s || !s_filter || nz <= 0 || nx <= 0) {
+        fprintf(stderr, "<error>: %s: invalid input (nz=%d, nx=%d)\n", name, nz, nx);
+        return;
+    }
+    if (!(kpass > 0.0f) || kcut <= kpass) {
+        fprintf(stderr, "<error>: %s: need 0 < kpass < kcut (kpass=%g, kcut=%g)\n", name, kpass, kcut);
+        return;
+    }
+    // taper lengths and pad as lowpass2d (common.c:1079-1091); taper_traces clamps to a third
+    const int Lx = (int)roundf(4 / (kpass * dx)), Lz = (int)roundf(4 / (kpass * dz));
+    const int pad = 10 * (Lx > Lz ? Lx : Lz);
+    const int Lt = Lz > nz / 3 ? nz / 3 : Lz, Lr = Lx > nx / 3 ? nx / 3 : Lx;
+    const long long Nz = nz + 2LL * pad, Nx = nx + 2LL * pad;
+    if (Nz * Nx > (1LL << 31) / 2) {
+        fprintf(stderr, "<error>: %s: padded field %lld x %lld too large\n", name, Nz, Nx);
+        return;
+    }
+    std::vector<float> tct(Lt + 1), tcr(Lr + 1);
+    if (Lt > 0) fwi_taper_coefs(Lt, tct.data());
+    if (Lr > 0) fwi_taper_coefs(Lr, tcr.data());
+    const size_t m = (size_t)nz * nx, plane = (size_t)(Nz * Nx);
+    const size_t bx = al(m * 4), bT = al((size_t)Nz * 2 * nx * 4), bF = al(2 * plane * 4), bV = bT;
+    const size_t bt = al((Lt + 1) * 4) + al((Lr + 1) * 4);
+    if (!ops_ready(2 * bx + bT + bF + bV + bt + al(sizeof(TaperDesc)) + 256) || !blas_ready()) return;
+    char *b = g_ops.buf;
+    float *x = (float *)b, *T = (float *)(b + bx), *F = (float *)(b + bx + bT), *V = (float *)(b + bx + bT + bF);
+    float *Y = (float *)(b + bx + bT + bF + bV);
+    float *dct = (float *)(b + 2 * bx + bT + bF + bV), *dcr = (float *)((char *)dct + al((Lt + 1) * 4));
+    TaperDesc *td = (TaperDesc *)(b + 2 * bx + bT + bF + bV + bt);
+
+    const int iNx = (int)Nx, iNz = (int)Nz;
+    const int wi[3] = {filter, iNx, iNz}, zi[2] = {nz, pad}, xi[2] = {nx, pad};
+    const float wf[4] = {dx, dz, kpass, kcut};
+    const std::string sz = "/" + std::to_string(nz) + "/" + std::to_string(pad), sx = "/" + std::to_string(nx) + "/" +
+                                                                                    std::to_string(pad);
+    const float *Wd = op_matrix("w2/" + std::to_string(filter) + "/" + std::to_string(iNx) + "/" +
+                                    std::to_string(iNz) + "/" + fbits(dx) + "/" + fbits(dz) + "/" + fbits(kpass) +
+                                    "/" + fbits(kcut),
+                                plane, build_wn_window, wi, wf);
+    const float *Az = op_matrix("wfz" + sz, 2 * (size_t)Nz * nz, build_wn_fz, zi, nullptr);
+    const float *Rf = op_matrix("wfx" + sx, 4 * (size_t)Nx * nx, build_wn_fx, xi, nullptr);
+    const float *Ri = op_matrix("wix" + sx, 4 * (size_t)Nx * nx, build_wn_ix, xi, nullptr);
+    const float *Lz_ = op_matrix("wiz" + sz, 2 * (size_t)Nz * nz, build_wn_iz, zi, nullptr);
+    if (!Wd || !Az || !Rf || !Ri || !Lz_) return;
+
+    cudaMemcpyAsync(x, s[0], m * 4, cudaMemcpyHostToDevice, g_ops.st);
+    cudaMemcpyAsync(dct, tct.data(), (Lt + 1) * 4, cudaMemcpyHostToDevice, g_ops.st);
+    cudaMemcpyAsync(dcr, tcr.data(), (Lr + 1) * 4, cudaMemcpyHostToDevice, g_ops.st);
+    if (!taper_device(x, nz, nx, Lt, Lr, dct, dcr, td)) return;
+    cudaMemcpyAsync(s[0], x, m * 4, cudaMemcpyDeviceToHost, g_ops.st);  // the reference tapers its input
+
+    const float one = 1.0f, zero = 0.0f, inv = 1.0f / (float)(Nz * Nx);
+    bool ok =
+        // [Tr | Ti] = [C'z X | -S'z X]                                         (Nz x 2nx)
+        cublasSgemmStridedBatched(g_blas, CUBLAS_OP_N, CUBLAS_OP_N, iNz, nx, nz, &one, Az, iNz, (long long)Nz * nz, x,
+                                  nz, 0, &zero, T, iNz, (long long)Nz * nx, 2) == CUBLAS_STATUS_SUCCESS &&
+        // [Fr | Fi] = [Tr | Ti] [[C'x^T, -S'x^T], [S'x^T, C'x^T]]               (Nz x 2Nx)
+        cublasSgemm(g_blas, CUBLAS_OP_N, CUBLAS_OP_N, iNz, 2 * iNx, 2 * nx, &one, T, iNz, Rf, 2 * nx, &zero, F, iNz) ==
+            CUBLAS_STATUS_SUCCESS;
+    if (ok) {
+        k_window2<<<592, 256, 0, g_ops.st>>>(F, Wd, (long long)plane);
+        ok = report(cudaGetLastError(), "k_window2");
+    }
+    ok = ok &&
+         // Vr, Vi = [Gr | Gi] times the two column blocks of the inverse x operator, stacked (2Nz x nx)
+         cublasSgemm(g_blas, CUBLAS_OP_N, CUBLAS_OP_N, iNz, nx, 2 * iNx, &one, F, iNz, Ri, 2 * iNx, &zero, V,
+                     2 * iNz) == CUBLAS_STATUS_SUCCESS &&
+         cublasSgemm(g_blas, CUBLAS_OP_N, CUBLAS_OP_N, iNz, nx, 2 * iNx, &one, F, iNz, Ri + 2 * Nx * nx, 2 * iNx,
+                     &zero, V + Nz, 2 * iNz) == CUBLAS_STATUS_SUCCESS &&
+         // Y = [Cz | -Sz] [Vr; Vi] / (Nz Nx) at the kept rows                    (nz x nx)
+         cublasSgemm(g_blas, CUBLAS_OP_N, CUBLAS_OP_N, nz, nx, 2 * iNz, &inv, Lz_, nz, V, 2 * iNz, &zero, Y, nz) ==
+             CUBLAS_STATUS_SUCCESS;
+    if (!ok) {
+        fprintf(stderr, "<error>: %s: GEMM failed\n", name);
+        cudaStreamSynchronize(g_ops.st);
+        return;
+    }
+    cudaMemcpyAsync(s_filter[0], Y, m * 4, cudaMemcpyDeviceToHost, g_ops.st);
+    report(cudaStreamSynchronize(g_ops.st), name);
+}
+
+}  // namespace
+
+extern "C" void lowpass2d(float **s, int nz, int nx, float dz, float dx, float kpass, float kcut, float **s_filter)
+{
+    wavenumber_filter(s, nz, nx, dz, dx, kpass, kcut, s_filter, 0, "lowpass2d");
+}
+
+extern "C" void bandpass2d(float **s, int nz, int nx, float dz, float dx, float kpass, float kcut, float **s_filter)
+{
+    wavenumber_filter(s, nz, nx, dz, dx, kpass, kcut, s_filter, 1, "bandpass2d");
+}
+
 // apply_gradient_shot_precondition, optimization.c:58-97
 extern "C" void apply_gradient_shot_precondition(float *grad, float *precond, int n)
 {

@@ -371,3 +371,159 @@ void fwi_interp_operator(int ns, int r, int nt, float *M)
     free(g);
     free(cs);
 }
+
+/* ------------------------------------------------------------ 2-D wavenumber filters */
+/* generate_frequency (common.c:333-361): angular frequencies of an n-point FFT, float */
+static void angular_frequency(float *f, float d, int n)
+{
+    const float df = 2.0f * (float)3.141592653589793 / (n * d);
+    const int nf = n / 2 + 1;
+    f[0] = 0.0f;
+    for (int it = 1; it < nf; it++) {
+        f[it] = it * df;
+        if (n - it >= nf) f[n - it] = -f[it];
+    }
+}
+
+void fwi_wavenumber_window(int filter, int Nx, int Nz, float dx, float dz, float kpass, float kcut, float *W)
+{
+    float *kx = (float *)malloc(sizeof(float) * (size_t)Nx), *kz = (float *)malloc(sizeof(float) * (size_t)Nz);
+    angular_frequency(kx, dx, Nx);
+    angular_frequency(kz, dz, Nz);
+    const float pi = (float)3.141592653589793;
+    for (int ix = 0; ix < Nx; ix++)
+        for (int iz = 0; iz < Nz; iz++) {
+            /* the reference evaluates iz <= Nz/2 and lets c2r mirror the rest; |KX|, |KZ| of the
+             * mirrored entries are the same floats, so evaluating every entry is identical */
+            const float KX = kx[ix] / (2.0f * pi), KZ = kz[iz] / (2.0f * pi);
+            const float k = sqrtf(KX * KX + KZ * KZ);
+            float w;
+            if (filter == 0) {
+                const float taperLen = kcut - kpass;
+                if (k < kpass) w = 1.0f;
+                else if (k >= kpass && k <= kcut) w = 0.5f * (1.0f + cosf(pi * (k - kpass) / taperLen));
+                else w = 0.0f;
+            } else {
+                const float lo = kpass, hi = kcut - kpass;
+                if (k < kpass) w = 0.5f * (1.0f + cosf(pi * (kpass - k) / lo));
+                else if (k >= kpass && k <= kcut) w = 0.5f * (1.0f + cosf(pi * (k - kpass) / hi));
+                else w = 0.0f;
+            }
+            W[(size_t)ix * Nz + iz] = w;
+        }
+    free(kx);
+    free(kz);
+}
+
+/* cos and sin of 2 pi m / n, m = 0..n-1, FP64; entry (a b mod n) gives the DFT matrix element */
+typedef struct { double *c, *s; int n; } dft_table;
+
+static dft_table dft_table_make(int n)
+{
+    dft_table t = {(double *)malloc(sizeof(double) * (size_t)n), (double *)malloc(sizeof(double) * (size_t)n), n};
+    for (int m = 0; m < n; m++) {
+        t.c[m] = cos(2.0 * 3.141592653589793 * m / n);
+        t.s[m] = sin(2.0 * 3.141592653589793 * m / n);
+    }
+    return t;
+}
+
+static void dft_table_free(dft_table *t)
+{
+    free(t->c);
+    free(t->s);
+}
+
+static void dft_cs(const dft_table *t, long long a, long long b, double *c, double *sn)
+{
+    const int m = (int)((a * b) % t->n);
+    *c = t->c[m];
+    *sn = t->s[m];
+}
+
+/* padded index p of an n-sample line padded by `pad` replicated edge samples on each side */
+static int pad_source(int p, int pad, int n)
+{
+    int q = p - pad;
+    return q < 0 ? 0 : (q >= n ? n - 1 : q);
+}
+
+void fwi_wn_forward_z(int nz, int pad, float *A)
+{
+    const int Nz = nz + 2 * pad;
+    dft_table t = dft_table_make(Nz);
+    double *c = (double *)calloc((size_t)Nz * nz, sizeof(double)), *sn = (double *)calloc((size_t)Nz * nz, sizeof(double));
+    for (int p = 0; p < Nz; p++) {
+        const int b = pad_source(p, pad, nz);
+        for (int a = 0; a < Nz; a++) {
+            double cv, sv;
+            dft_cs(&t, a, p, &cv, &sv);
+            c[(size_t)b * Nz + a] += cv;
+            sn[(size_t)b * Nz + a] += sv;
+        }
+    }
+    for (size_t i = 0; i < (size_t)Nz * nz; i++) {
+        A[i] = (float)c[i];
+        A[(size_t)Nz * nz + i] = (float)-sn[i];
+    }
+    free(c);
+    free(sn);
+    dft_table_free(&t);
+}
+
+void fwi_wn_forward_x(int nx, int pad, float *R)
+{
+    const int Nx = nx + 2 * pad, ld = 2 * nx;
+    dft_table t = dft_table_make(Nx);
+    double *c = (double *)calloc((size_t)Nx * nx, sizeof(double)), *sn = (double *)calloc((size_t)Nx * nx, sizeof(double));
+    for (int p = 0; p < Nx; p++) {
+        const int b = pad_source(p, pad, nx);
+        for (int q = 0; q < Nx; q++) {
+            double cv, sv;
+            dft_cs(&t, q, p, &cv, &sv);
+            c[(size_t)q * nx + b] += cv; /* Cx' transposed: [b][q] at q * nx + b */
+            sn[(size_t)q * nx + b] += sv;
+        }
+    }
+    for (int q = 0; q < Nx; q++)
+        for (int b = 0; b < nx; b++) {
+            const float cv = (float)c[(size_t)q * nx + b], sv = (float)sn[(size_t)q * nx + b];
+            R[(size_t)q * ld + b] = cv;             /* [[C', -S'], [S', C']], column q < Nx */
+            R[(size_t)q * ld + nx + b] = sv;
+            R[(size_t)(Nx + q) * ld + b] = -sv;
+            R[(size_t)(Nx + q) * ld + nx + b] = cv;
+        }
+    free(c);
+    free(sn);
+    dft_table_free(&t);
+}
+
+void fwi_wn_inverse_x(int nx, int pad, float *R)
+{
+    const int Nx = nx + 2 * pad, ld = 2 * Nx;
+    dft_table t = dft_table_make(Nx);
+    for (int j = 0; j < nx; j++)
+        for (int q = 0; q < Nx; q++) {
+            double cv, sv;
+            dft_cs(&t, j + pad, q, &cv, &sv);
+            R[(size_t)j * ld + q] = (float)cv;              /* [[C^T, S^T], [-S^T, C^T]], column j < nx */
+            R[(size_t)j * ld + Nx + q] = (float)-sv;
+            R[(size_t)(nx + j) * ld + q] = (float)sv;
+            R[(size_t)(nx + j) * ld + Nx + q] = (float)cv;
+        }
+    dft_table_free(&t);
+}
+
+void fwi_wn_inverse_z(int nz, int pad, float *L)
+{
+    const int Nz = nz + 2 * pad;
+    dft_table t = dft_table_make(Nz);
+    for (int p = 0; p < Nz; p++)
+        for (int i = 0; i < nz; i++) {
+            double cv, sv;
+            dft_cs(&t, i + pad, p, &cv, &sv);
+            L[(size_t)p * nz + i] = (float)cv;               /* [C | -S] */
+            L[(size_t)(Nz + p) * nz + i] = (float)-sv;
+        }
+    dft_table_free(&t);
+}

@@ -120,6 +120,16 @@ FWI_API void apply_traces_lowpass(float **tr, float **trs, int nt, int ntr, floa
 FWI_API void apply_traces_bandpass(float **tr, float **trs, int nt, int ntr, float fpass, float fcut, float dt);
 FWI_API void interpolate_traces(float **tr, int ntr, int nt, int r, float **trs);
 
+/* common.c:1042-1162 / :1164-1284 (common.h): the 2-D wavenumber low/band-pass of an nz x nx field
+ * (s[ix][iz], alloc2float(nz, nx)).  As the reference: the cosine taper of taper_traces with
+ * lengths roundf(4 / (kpass d)) is applied to s IN PLACE, the field is padded by 10 x the longer
+ * taper with replicated edges, transformed, multiplied by the radial cosine window between kpass
+ * and kcut (1/m), transformed back, / (Nz Nx) and cropped into s_filter (which may be s).  On the
+ * GPU as FP32 GEMMs with DFT operators that fold the pad and the crop (within 1e-5 relative of
+ * the FFTs).  kcut <= kpass or kpass <= 0 prints an error and leaves both arrays unchanged. */
+FWI_API void lowpass2d(float **s, int nz, int nx, float dz, float dx, float kpass, float kcut, float **s_filter);
+FWI_API void bandpass2d(float **s, int nz, int nx, float dz, float dx, float kpass, float kcut, float **s_filter);
+
 /* replace the optimization.h reductions (optimization.c:13-298), computed on the device */
 FWI_API void apply_gradient_precondition(float *grad, const float *precond, int n, float alpha);
 FWI_API void apply_gradient_shot_precondition(float *grad, float *precond, int n);

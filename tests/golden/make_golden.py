@@ -113,6 +113,30 @@ def case(name, nz, nx, nt, dt, pml, fs, nshot, seed, problems=(0, 1, 2), precond
     print(f"{name}: {os.path.getsize(path) / 1024:.0f} KiB")
 
 
+def wavenumber_case():
+    """lowpass2d / bandpass2d (common.c:1042-1284, defined but not called by the reference's
+    engine) on a seeded gradient-like field; the reference tapers its input in place, which
+    the fixture records as well."""
+    import ctypes as C
+    ref = po.Reference("strict")
+    L = ref.lib
+    nz, nx, dz, dx = 40, 70, 12.5, 10.0
+    rng = np.random.default_rng(13)
+    base = M.smooth_model(rng.standard_normal((nx, nz)).astype(np.float32) * 100.0 + 2000.0, 2.0).astype(np.float32)
+    out = dict(field=base, nz=nz, nx=nx, dz=np.float32(dz), dx=np.float32(dx))
+    for name, fn, kpass, kcut in (("low", L.lowpass2d, 0.02, 0.04), ("band", L.bandpass2d, 0.015, 0.035)):
+        s = base.copy()
+        y = np.zeros_like(s)
+        fn(po.rows(s), nz, nx, C.c_float(dz), C.c_float(dx), C.c_float(kpass), C.c_float(kcut), po.rows(y))
+        out[f"{name}_kpass"] = np.float32(kpass)
+        out[f"{name}_kcut"] = np.float32(kcut)
+        out[f"{name}_out"] = y
+        out[f"{name}_tapered_input"] = s
+    path = os.path.join(HERE, "aux_wavenumber.npz")
+    np.savez_compressed(path, **out)
+    print(f"aux_wavenumber: {os.path.getsize(path) / 1024:.0f} KiB")
+
+
 def main():
     if not po.ref_available("strict"):
         if not po.build_ref():
@@ -140,6 +164,8 @@ def main():
     # (interpolate_traces, common.c:482-582), with and without the lowpass
     case("sr2_grad", 36, 60, 301, 0.001, 7, 1, 2, seed=11, sr=2)
     case("sr2_filt0", 36, 60, 301, 0.001, 7, 1, 2, seed=12, problems=(0, 1), sr=2, filt=0.0)
+    if not only or "wavenumber" in only:
+        wavenumber_case()
 
 
 if __name__ == "__main__":
