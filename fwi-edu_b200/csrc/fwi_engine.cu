@@ -138,6 +138,7 @@ struct fwi_ctx {
     fwi_stats stats{};
     int math = 0;  // 0: bit-exact arithmetic, 1: contracted multiply-adds
     bool use_graphs = true;  // capture the batched launch sequences as CUDA graphs
+    bool pdl = true;         // consecutive steps as programmatic dependent launches
     bool tune = true;        // time the step kernel's launch shapes once per shape (autotune)
     int last_tx = 0, last_nst = 0, last_chunk = 0, last_gpt = 0;  // the shape of the last launch
     int *d_err = nullptr;  // set by a step kernel whose tile copy did not complete
@@ -226,6 +227,7 @@ extern "C" int fwi_ctx_create(fwi_ctx **out, int device, size_t budget)
     c->budget = budget;
     if (const char *e = getenv("FWI_MATH")) c->math = atoi(e) ? 1 : 0;
     if (const char *e = getenv("FWI_GRAPH")) c->use_graphs = e[0] != '0';  // 0: direct launches (profilers)
+    if (const char *e = getenv("FWI_PDL")) c->pdl = e[0] != '0';
     if (const char *e = getenv("FWI_TUNE")) c->tune = e[0] != '0';            // 0: heuristic launch shapes
     CK(cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking));
     CK(cudaEventCreate(&c->ev0));
@@ -851,11 +853,23 @@ static int launch_tiles(fwi_ctx *c, const Program *prog, int L0, int L1, int sho
     CUtensorMap m1, m0, mc;
     if (tx == 16) TRY(encode_group_maps<16>(r0->d, nshot, p->d_coef, &m1, &m0, &mc));
     else TRY(encode_group_maps<8>(r0->d, nshot, p->d_coef, &m1, &m0, &mc));
+    // each step may launch while the previous one drains: its blocks set up barriers and
+    // per-shot scalars, then wait (griddepcontrol.wait) before touching any field
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    attr[0].val.programmaticStreamSerializationAllowed = 1;
+    cudaLaunchConfig_t lc = {};
+    lc.gridDim = grid;
+    lc.blockDim = dim3(nl, tx + 32 / nl);
+    lc.dynamicSmemBytes = smem;
+    lc.stream = c->stream;
+    lc.attrs = attr;
+    lc.numAttrs = c->pdl ? 1 : 0;
     for (int L = L0; L < L1; L++) {
         const int4 &pw = prog->items[L];
         if (pw.x == K_NONE && pw.z == K_NONE) continue;
-        fn<<<grid, dim3(nl, tx + 32 / nl), smem, c->stream>>>(m1, m0, mc, c->d_desc, prog->d, L, shot_base, nshot,
-                                                               chunk, c->d_err);
+        CK(cudaLaunchKernelEx(&lc, fn, m1, m0, mc, (const ShotDesc *)c->d_desc, (const int4 *)prog->d, L, shot_base,
+                              nshot, chunk, c->d_err));
         c->launches++;
     }
     CK(cudaGetLastError());

@@ -188,6 +188,25 @@ __device__ __forceinline__ bool mbar_wait(unsigned bar, unsigned parity)
         if (global_ns() - t0 > 2000000000ull) return false;
     }
 }
+// programmatic dependent launch: a step may start (launch its blocks, set up barriers and
+// per-shot scalars) while the previous step drains; every access to the fields waits for the
+// previous step to complete.  Without the launch attribute both are no-ops.
+__device__ __forceinline__ void grid_dep_launch() { asm volatile("griddepcontrol.launch_dependents;" ::: "memory"); }
+__device__ __forceinline__ void grid_dep_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
+
+// frames read (p1 = t, p0) and written by a step of the given kind
+__device__ __forceinline__ void step_frames(const ShotDesc &D, int kind, int it, int &i1, int &i0, int &io)
+{
+    if (kind == K_FWD0 || kind == K_FWD1) {
+        const bool keep = kind == K_FWD1;
+        i1 = fwd_idx(D, it, keep); i0 = fwd_idx(D, it - 1, keep); io = fwd_idx(D, it + 1, keep);
+    } else if (kind == K_REP) {
+        i1 = rep_idx(D, it); i0 = rep_idx(D, it - 1); io = rep_idx(D, it + 1);
+    } else {
+        i1 = adj_idx(D, it); i0 = adj_idx(D, it + 1); io = adj_idx(D, it - 1);
+    }
+}
+
 // tile copies global -> this CTA's shared memory, completing on bar (no multicast); the
 // tensor maps are __grid_constant__ kernel parameters
 __device__ __forceinline__ void tma_load3(unsigned dst, const CUtensorMap *m, int c0, int c1, int c2, unsigned bar)
@@ -253,6 +272,7 @@ __global__ void __launch_bounds__(TG / GPT * TX + 32)
     __shared__ bool s_spec[TILE_CH_MAX];
     __shared__ int s_fi[2];  // frames of p1 and p0 (the same for every shot of the chunk)
 
+    grid_dep_launch();  // the next step may begin its set-up once every block of this one runs
     const int4 pw = prog[L];
     const int kind = (blockIdx.y & 1) ? pw.z : pw.x;
     const int it = (blockIdx.y & 1) ? pw.w : pw.y;
@@ -270,6 +290,7 @@ __global__ void __launch_bounds__(TG / GPT * TX + 32)
     // ---- the receiver-sampling block: p1 is read-only during this launch
     if ((int)blockIdx.x >= ntx) {
         if (!fwd || it % A.sr != 0 || (int)blockIdx.x > ntx || blockIdx.z != 0) return;
+        grid_dep_wait();
         for (int s = 0; s < n; ++s) {
             const ShotDesc &D = shots[cb + s];
             const float *p1 = fwd_buf(D, it, kind == K_FWD1);
@@ -279,19 +300,39 @@ __global__ void __launch_bounds__(TG / GPT * TX + 32)
         return;
     }
 
-    // ---- per-shot scalars of the chunk (frame indices need divisions: once per block)
-    if (tid < n) {
+    const int X0 = blockIdx.x * TX, G0 = blockIdx.z * TG;
+    unsigned char *st_base = smem + Geo::ST_OFF;
+    const bool producer = warp == NW && lane == 0;
+    int issued = 0;  // shots whose copies the producer has issued
+    if (producer) {
+        // ---- barriers, then the coefficient tile and the first NST shots' copies at once: the
+        // copies are in flight while the consumers compute the per-shot scalars
+        for (int j = 0; j < NST; ++j) {
+            mbar_init(smem_u32(&full[j]), 1);
+            mbar_init(smem_u32(&empty[j]), NW);
+        }
+        mbar_init(smem_u32(&cfbar), 1);
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+        int i1, i0, io;
+        step_frames(A, kind, it, i1, i0, io);  // the same frames for every shot of the chunk
+        s_fi[0] = i1;
+        s_fi[1] = i0;
+        grid_dep_wait();
+        mbar_arrive_expect(smem_u32(&cfbar), Geo::CF_BYTES);
+        tma_load3(smem_u32(smem), &tm_cf, 4 * G0, X0, 0, smem_u32(&cfbar));
+        for (; issued < min(n, NST); ++issued) {
+            const unsigned b = smem_u32(&full[issued]);
+            mbar_arrive_expect(b, Geo::P1_BYTES + Geo::P0_BYTES);
+            unsigned char *stg = st_base + issued * Geo::STAGE;
+            tma_load4(smem_u32(stg), &tm_p1, 4 * (G0 - 1), X0 - 3, i1, cb + issued - shot_base, b);
+            tma_load4(smem_u32(stg + Geo::P0_OFF), &tm_p0, 4 * G0, X0, i0, cb + issued - shot_base, b);
+        }
+    } else if (tid < n) {
+        // ---- per-shot scalars of the chunk (frame indices need divisions: once per block)
         const ShotDesc &D = shots[cb + tid];
         int i1, i0, io, iu = -1;
-        if (fwd) {
-            const bool keep = kind == K_FWD1;
-            i1 = fwd_idx(D, it, keep); i0 = fwd_idx(D, it - 1, keep); io = fwd_idx(D, it + 1, keep);
-        } else if (kind == K_REP) {
-            i1 = rep_idx(D, it); i0 = rep_idx(D, it - 1); io = rep_idx(D, it + 1);
-        } else {
-            i1 = adj_idx(D, it); i0 = adj_idx(D, it + 1); io = adj_idx(D, it - 1);
-            if (it % MST == 0) iu = img_idx(D, it);
-        }
+        step_frames(D, kind, it, i1, i0, io);
+        if (kind == K_ADJ && it % MST == 0) iu = img_idx(D, it);
         s_out[tid] = frame_ptr(D, io);
         s_u[tid] = iu >= 0 ? frame_ptr(D, iu) : nullptr;
         s_isx[tid] = D.isx;
@@ -307,32 +348,16 @@ __global__ void __launch_bounds__(TG / GPT * TX + 32)
                            D.isz < Z0t + 4 * TG;
         const bool inj_t = kind == K_ADJ && it >= 1 && Z0t + 4 * TG > D.rz0 && Z0t <= D.rz1;
         s_spec[tid] = src_t || inj_t;
-        if (tid == 0) {
-            s_fi[0] = i1;
-            s_fi[1] = i0;
-        }
-    }
-    if (tid == 0) {
-        for (int j = 0; j < NST; ++j) {
-            mbar_init(smem_u32(&full[j]), 1);
-            mbar_init(smem_u32(&empty[j]), NW);
-        }
-        mbar_init(smem_u32(&cfbar), 1);
-        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
     __syncthreads();  // barriers and the per-shot scalars; no block-wide barrier follows
-    const int X0 = blockIdx.x * TX, G0 = blockIdx.z * TG;
-    unsigned char *st_base = smem + Geo::ST_OFF;
+    grid_dep_wait();  // fields and accumulators: after the previous step (the producer waited already)
 
     if (warp == NW) {
-        // ---- producer: coefficients once, then shot j into stage j % NST once every
-        // consumer warp has released that stage's previous shot
+        // ---- producer: shot j into stage j % NST once every consumer warp has released that
+        // stage's previous shot
         if (lane != 0) return;
-        mbar_arrive_expect(smem_u32(&cfbar), Geo::CF_BYTES);
-        tma_load3(smem_u32(smem), &tm_cf, 4 * G0, X0, 0, smem_u32(&cfbar));
         const int i1 = s_fi[0], i0 = s_fi[1];
-        int issued = 0;
-        for (int j = 0; j < n; ++j) {
+        for (int j = issued; j < n; ++j) {
             const int st = j % NST;
             if (j >= NST && !mbar_wait(smem_u32(&empty[st]), (j / NST - 1) & 1)) {
                 atomicExch(err, 1);
