@@ -554,7 +554,6 @@ static int prepare_run(fwi_ctx *c, ShotRun *r, int shot, bool gradient)
     d.isx = s.isx + c->pml; d.isz = s.isz + c->pml;
     d.invdx = hc.invdx; d.invdz = hc.invdz; d.invdxdx = hc.invdxdx; d.invdzdz = hc.invdzdz;
     d.invdtdt = hc.invdtdt; d.dt = c->dt;
-    d.negzero = -0.0f;
     const size_t fr = p->frame();
     d.frame = (long long)fr;
     d.c1 = p->d_coef; d.c2 = p->d_coef + fr; d.ck = p->d_coef + 2 * fr;

@@ -27,7 +27,6 @@ struct ShotDesc {
     int nt, d, K, ns, sr, ntr, S5, hessian;
     int isx, isz;  // padded source cell
     float invdx, invdz, invdxdx, invdzdz, invdtdt, dt;
-    float negzero;  // -0.0f, read at run time (the exact packed products are fma(a, b, -0))
     // coefficients [Nx][ld]
     const float *c1, *c2, *ck, *irx, *irz, *ir;
     // source terms per step: forward (double, propagation.c:558) and replay (float, :662)

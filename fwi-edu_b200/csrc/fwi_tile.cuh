@@ -75,13 +75,12 @@ __device__ __forceinline__ u64 fma2(u64 a, u64 b, u64 c)
     return d;
 }
 
-// stencil constants (propagation.h) and grid spacings as packed pairs.  nz holds -0.0 in
-// both halves, loaded at run time: the exact path forms every product as fma(a, b, nz),
-// which is round(a*b) bit for bit.  A plain packed multiply would be fused by the
-// compiler into a following packed add (one rounding instead of two) although both carry
-// .rn; an addend it cannot see is -0 keeps each product a separate, rounded step.
+// stencil constants (propagation.h) and grid spacings as packed pairs.  The exact path rounds
+// every product on its own with two scalar multiplies (__fmul_rn is never contracted); a
+// packed multiply would be fused by the compiler into the following packed add (one rounding
+// instead of two) although both carry .rn.  The sums stay packed.
 struct PkConst {
-    u64 C1, C2, C3, D0, D1, D2, D3, idx, idz, idxx, idzz, nz;
+    u64 C1, C2, C3, D0, D1, D2, D3, idx, idz, idxx, idzz;
 };
 
 // two vertically adjacent cells of one column: propagation.c:13-74 with each product and
@@ -92,7 +91,10 @@ __device__ __forceinline__ u64 cell2(u64 zm3, u64 zm2, u64 zm1, u64 z0, u64 zp1,
                                      u64 ir, u64 p0, const PkConst &k)
 {
     if (MATH == 0) {
-        auto mul = [&](u64 a, u64 b) { return fma2(a, b, k.nz); };
+        auto mul = [&](u64 a, u64 b) {
+            const float2 x = upk(a), y = upk(b);
+            return pk(__fmul_rn(x.x, y.x), __fmul_rn(x.y, y.y));
+        };
         const u64 dpdz = mul(add2(add2(mul(k.C1, sub2(zp1, zm1)), mul(k.C2, sub2(zp2, zm2))), mul(k.C3, sub2(zp3, zm3))),
                              k.idz);
         const u64 dpdx = mul(add2(add2(mul(k.C1, sub2(xp1, xm1)), mul(k.C2, sub2(xp2, xm2))), mul(k.C3, sub2(xp3, xm3))),
@@ -187,6 +189,14 @@ __device__ __forceinline__ bool mbar_wait(unsigned bar, unsigned parity)
         if (mbar_try(bar, parity)) return true;
         if (global_ns() - t0 > 2000000000ull) return false;
     }
+}
+// a 16-byte shared-memory load at a 32-bit shared address (volatile: never moved above the
+// barrier wait that guards the stage it reads)
+__device__ __forceinline__ float4 lds4(unsigned a)
+{
+    float4 v;
+    asm volatile("ld.shared.v4.f32 {%0, %1, %2, %3}, [%4];" : "=f"(v.x), "=f"(v.y), "=f"(v.z), "=f"(v.w) : "r"(a));
+    return v;
 }
 // programmatic dependent launch: a step may start (launch its blocks, set up barriers and
 // per-shot scalars) while the previous step drains; every access to the fields waits for the
@@ -409,24 +419,24 @@ __global__ void __launch_bounds__(TG / GPT * TX + 32)
     K.idz = pk(invdz, invdz);
     K.idxx = pk(A.invdxdx, A.invdxdx);
     K.idzz = pk(A.invdzdz, A.invdzdz);
-    K.nz = pk(A.negzero, A.negzero);
     const float4 zero4 = make_float4(0.f, 0.f, 0.f, 0.f);
     const float4(*scf)[TX][TG] = reinterpret_cast<const float4(*)[TX][TG]>(smem);
     float4 cfh[6];  // one group per thread: its coefficients stay in registers for the chunk
 
     // group gl of the tile for shot i: stencil from the stage, fused epilogue, store;
     // lo / cq / hi are groups gl-1, gl, gl+1 of column x
-    auto consume_group = [&](int i, const float4 (*sp1)[TG + 2], const float4 (*sp0)[TG], int gl, const float4 &lo,
+    auto consume_group = [&](int i, unsigned sb, int gl, const float4 &lo,
                              const float4 &cq, const float4 &hi) {
         const int g = G0 + gl, z0 = 4 * g;
         if (g >= G || !xin) return;
         const int cx = k + 3, cg = gl + 1;
         const bool zfd = z0 + 3 >= zlo && z0 <= zhi;
-        const float4 p0 = sp0[k][gl];
+        const float4 p0 = lds4(sb + Geo::P0_OFF + (unsigned)(k * TG + gl) * 16u);
         float4 v = zero4;
         if (zfd && xint) {
-            const float4 xn[6] = {sp1[cx - 3][cg], sp1[cx - 2][cg], sp1[cx - 1][cg],
-                                  sp1[cx + 1][cg], sp1[cx + 2][cg], sp1[cx + 3][cg]};
+            const unsigned xa = sb + (unsigned)(cx * (TG + 2) + cg) * 16u, cs = (TG + 2) * 16u;
+            const float4 xn[6] = {lds4(xa - 3 * cs), lds4(xa - 2 * cs), lds4(xa - cs),
+                                  lds4(xa + cs), lds4(xa + 2 * cs), lds4(xa + 3 * cs)};
             if (GPT == 1) {
                 v = group2<MATH>(lo, cq, hi, xn, cfh, p0, K);
             } else {
@@ -508,15 +518,15 @@ __global__ void __launch_bounds__(TG / GPT * TX + 32)
 
     // one shot of the chunk from ring stage st: the lane's GPT groups, sharing their z-window
     auto consume_shot = [&](int i, int st) {
-        const unsigned char *stg = st_base + st * Geo::STAGE;
-        const float4(*sp1)[TG + 2] = reinterpret_cast<const float4(*)[TG + 2]>(stg);
-        const float4(*sp0)[TG] = reinterpret_cast<const float4(*)[TG]>(stg + Geo::P0_OFF);
+        // stage st as a 32-bit shared address: p1 tile [XP][TG + 2] float4, then p0 [TX][TG]
+        const unsigned sb = smem_u32(st_base) + (unsigned)(st * Geo::STAGE);
         const int gl0 = GPT * zl;
         float4 w[GPT + 2];  // groups gl0-1 .. gl0+GPT of column x (stage rows gl0 .. gl0+GPT+1)
+        const unsigned wa = sb + (unsigned)((k + 3) * (TG + 2) + gl0) * 16u;
 #pragma unroll
-        for (int q = 0; q < GPT + 2; ++q) w[q] = sp1[k + 3][gl0 + q];
+        for (int q = 0; q < GPT + 2; ++q) w[q] = lds4(wa + 16u * q);
 #pragma unroll
-        for (int j = 0; j < GPT; ++j) consume_group(i, sp1, sp0, gl0 + j, w[j], w[j + 1], w[j + 2]);
+        for (int j = 0; j < GPT; ++j) consume_group(i, sb, gl0 + j, w[j], w[j + 1], w[j + 2]);
     };
 
     {  // coefficient tiles, once for all shots
