@@ -1497,6 +1497,42 @@ static int run_gradient_group(fwi_ctx *c, std::vector<ShotRun *> &rs, float freq
     return FWI_OK;
 }
 
+// Shots per wave of the batched path: all of them when the frame blocks of every group fit next
+// to what is allocated already (the reduction buffer is allocated first) and a reserve for what
+// a pass allocates later (descriptor scratch, programs, residual-filter operators): 1/16 of the
+// context's budget (at least 4 MiB), else 1/16 of the device.  Otherwise as many shots of the
+// largest frame block as fit.  FWI_WAVE caps the wave (the memory-bounded schedule on a small
+// survey).
+static const int WAVE_POOL = -2;
+static int wave_shots(fwi_ctx *c, const std::vector<std::pair<int, int>> &groups, int *out)
+{
+    TRY(ensure_red(c));
+    int ns = 0;
+    size_t need = 0, per_max = 0, pooled = 0;
+    for (auto &gr : groups) {
+        const ShotDesc &d = c->runs[gr.first]->d;
+        const size_t per = (size_t)d.nfr * (size_t)d.frame * 4;
+        need += per * (size_t)gr.second;
+        per_max = std::max(per_max, per);
+        ns += gr.second;
+    }
+    for (auto &kv : c->pools) pooled += kv.second.bytes;
+    size_t avail;
+    if (c->budget) {
+        avail = c->budget > c->used ? c->budget - c->used + pooled : pooled;
+        avail -= std::min(avail, std::max<size_t>(c->budget / 16, (size_t)4 << 20));
+    } else {
+        size_t fr = 0, tot = 0;
+        CK(cudaMemGetInfo(&fr, &tot));
+        avail = fr + pooled;
+        avail -= std::min(avail, tot / 16);
+    }
+    int wave = need <= avail ? ns : (int)std::max<size_t>(1, avail / std::max<size_t>(per_max, 1));
+    if (const char *e = getenv("FWI_WAVE")) wave = std::min(wave, std::max(1, atoi(e)));
+    *out = std::min(wave, ns);
+    return FWI_OK;
+}
+
 extern "C" int fwi_ctx_run(fwi_ctx *c, int problem, float freq, int filter, int precondition, int path)
 {
     if (!c) return fail(FWI_ERR_ARG, "NULL context");
@@ -1526,21 +1562,53 @@ extern "C" int fwi_ctx_run(fwi_ctx *c, int problem, float freq, int filter, int 
             if (groups.empty() || c->runs[i]->plan != c->runs[groups.back().first]->plan) groups.push_back({i, 1});
             else groups.back().second++;
         }
-        for (auto &gr : groups) {
-            std::vector<ShotRun *> rs;
-            for (int i = gr.first; i < gr.first + gr.second; i++) rs.push_back(c->runs[i].get());
-            TRY(assign_pool(c, gr.first, rs));
+        // Waves: when the frame blocks of the whole survey do not fit in the device memory left,
+        // the shots of each group run in waves of as many shots as fit, one after the other
+        // through one reused frame pool (a pass zeroes the frames it starts from).  Everything
+        // else a shot keeps -- traces, per-shot gradient window, accumulators -- stays allocated
+        // for the whole run, so the stack after the last wave sees every shot.
+        int wave = ns;
+        TRY(wave_shots(c, groups, &wave));
+        if (wave >= ns) {
+            auto wp = c->pools.find(WAVE_POOL);
+            if (wp != c->pools.end()) {
+                drop_graphs(c);
+                dfree(c, wp->second.p, wp->second.bytes);
+                c->pools.erase(wp);
+            }
+            for (auto &gr : groups) {
+                std::vector<ShotRun *> rs;
+                for (int i = gr.first; i < gr.first + gr.second; i++) rs.push_back(c->runs[i].get());
+                TRY(assign_pool(c, gr.first, rs));
+            }
+            for (int i = 0; i < ns; i++) descs[i] = c->runs[i]->d;
+            TRY(upload_descs(c, descs));
+        } else {
+            for (auto it = c->pools.begin(); it != c->pools.end();) {
+                if (it->first == WAVE_POOL) {
+                    ++it;
+                    continue;
+                }
+                drop_graphs(c);  // captured launches hold the released pool's tensor maps
+                dfree(c, it->second.p, it->second.bytes);
+                it = c->pools.erase(it);
+            }
         }
-        for (int i = 0; i < ns; i++) descs[i] = c->runs[i]->d;
-        TRY(upload_descs(c, descs));
-        for (auto &gr : groups) {
-            std::vector<ShotRun *> rs;
-            for (int i = gr.first; i < gr.first + gr.second; i++) rs.push_back(c->runs[i].get());
-            std::string gkey = std::to_string(gr.first) + "+" + std::to_string(gr.second) + "@" +
-                               std::to_string((long long)(intptr_t)rs[0]->plan);
-            if (gradient) TRY(run_gradient_group(c, rs, freq, filter, precondition, true, gkey, gr.first));
-            else TRY(run_forward_group(c, rs, problem, freq, filter, true, gkey, gr.first));
-        }
+        for (auto &gr : groups)
+            for (int w0 = gr.first; w0 < gr.first + gr.second; w0 += wave) {
+                const int m = std::min(wave, gr.first + gr.second - w0);
+                std::vector<ShotRun *> rs;
+                for (int i = w0; i < w0 + m; i++) rs.push_back(c->runs[i].get());
+                if (wave < ns) {
+                    TRY(assign_pool(c, WAVE_POOL, rs));
+                    for (int i = 0; i < ns; i++) descs[i] = c->runs[i]->d;
+                    TRY(upload_descs(c, descs));
+                }
+                std::string gkey = std::to_string(w0) + "+" + std::to_string(m) + "@" +
+                                   std::to_string((long long)(intptr_t)rs[0]->plan);
+                if (gradient) TRY(run_gradient_group(c, rs, freq, filter, precondition, true, gkey, w0));
+                else TRY(run_forward_group(c, rs, problem, freq, filter, true, gkey, w0));
+            }
         if (gradient) {
             std::vector<ShotRun *> all;
             for (auto &r : c->runs) all.push_back(r.get());
