@@ -31,6 +31,8 @@
 #pragma once
 #include <cuda.h>  // CUtensorMap, the encoded tensor-copy descriptor type
 
+#include <type_traits>
+
 #include "fwi_step.cuh"
 
 namespace fwi {
@@ -425,13 +427,14 @@ __global__ void __launch_bounds__(TG / GPT * TX + 32)
 
     // group gl of the tile for shot i: stencil from the stage, fused epilogue, store;
     // lo / cq / hi are groups gl-1, gl, gl+1 of column x
-    auto consume_group = [&](int i, unsigned sb, int gl, const float4 &lo,
-                             const float4 &cq, const float4 &hi) {
-        const int g = G0 + gl, z0 = 4 * g;
-        if (g >= G || !xin) return;
+    // the updated value of group gl (zero outside the updated rows and columns); p0: the
+    // group's previous field, which the general epilogue needs too
+    auto group_value = [&](unsigned sb, int gl, const float4 &lo, const float4 &cq, const float4 &hi,
+                           float4 &p0) {
+        const int z0 = 4 * (G0 + gl);
         const int cx = k + 3, cg = gl + 1;
         const bool zfd = z0 + 3 >= zlo && z0 <= zhi;
-        const float4 p0 = lds4(sb + Geo::P0_OFF + (unsigned)(k * TG + gl) * 16u);
+        p0 = lds4(sb + Geo::P0_OFF + (unsigned)(k * TG + gl) * 16u);
         float4 v = zero4;
         if (zfd && xint) {
             const unsigned xa = sb + (unsigned)(cx * (TG + 2) + cg) * 16u, cs = (TG + 2) * 16u;
@@ -451,12 +454,31 @@ __global__ void __launch_bounds__(TG / GPT * TX + 32)
                 if (z0 + 3 < zlo || z0 + 3 > zhi) v.w = 0.f;
             }
         }
+        return v;
+    };
+
+    // group gl of the tile for shot i, in a tile and shot that need none of the rare parts of
+    // the epilogue: the value and its store only
+    auto consume_group_fast = [&](int i, unsigned sb, int gl, const float4 &lo, const float4 &cq,
+                                  const float4 &hi) {
+        const int g = G0 + gl;
+        if (g >= G || !xin) return;
+        float4 p0;
+        const float4 v = group_value(sb, gl, lo, cq, hi, p0);
+        *reinterpret_cast<float4 *>(s_out[i] + colx + 4 * g) = v;
+    };
+
+    // group gl of the tile for shot i with the whole epilogue
+    auto consume_group = [&](int i, unsigned sb, int gl, const float4 &lo,
+                             const float4 &cq, const float4 &hi) {
+        const int g = G0 + gl, z0 = 4 * g;
+        if (g >= G || !xin) return;
+        // above the free surface (rows < pml): never updated, stored or accumulated; the
+        // mirrored rows pml-3..pml-1 are written by the groups that hold pml+1..pml+3
+        if (A.fs && z0 + 3 < pml) return;
+        float4 p0;
+        float4 v = group_value(sb, gl, lo, cq, hi, p0);
         const long long col = colx + z0;
-        // most tiles need none of the rare parts of the epilogue: decided per tile and shot
-        if (!(fs_tile || acc_tile || s_spec[i])) {
-            *reinterpret_cast<float4 *>(s_out[i] + col) = v;
-            return;
-        }
         const bool fs_top = A.fs && z0 <= fs_hi;  // the surface row, the mirror source rows, or above
         const int jpml = (pml >= z0 && pml < z0 + 4) ? pml - z0 : -1;
         const int isx = s_isx[i], isz = s_isz[i];
@@ -517,7 +539,9 @@ __global__ void __launch_bounds__(TG / GPT * TX + 32)
     };
 
     // one shot of the chunk from ring stage st: the lane's GPT groups, sharing their z-window
-    auto consume_shot = [&](int i, int st) {
+    // one shot of the chunk from ring stage st: the lane's GPT groups, sharing their z-window;
+    // FAST: the store-only epilogue
+    auto consume_shot = [&](int i, int st, auto fast) {
         // stage st as a 32-bit shared address: p1 tile [XP][TG + 2] float4, then p0 [TX][TG]
         const unsigned sb = smem_u32(st_base) + (unsigned)(st * Geo::STAGE);
         const int gl0 = GPT * zl;
@@ -526,9 +550,13 @@ __global__ void __launch_bounds__(TG / GPT * TX + 32)
 #pragma unroll
         for (int q = 0; q < GPT + 2; ++q) w[q] = lds4(wa + 16u * q);
 #pragma unroll
-        for (int j = 0; j < GPT; ++j) consume_group(i, sb, gl0 + j, w[j], w[j + 1], w[j + 2]);
+        for (int j = 0; j < GPT; ++j) {
+            if (decltype(fast)::value) consume_group_fast(i, sb, gl0 + j, w[j], w[j + 1], w[j + 2]);
+            else consume_group(i, sb, gl0 + j, w[j], w[j + 1], w[j + 2]);
+        }
     };
 
+    const bool rare_tile = fs_tile || acc_tile;
     {  // coefficient tiles, once for all shots
         bool ok = mbar_wait(smem_u32(&cfbar), 0);
         if (!__all_sync(0xffffffffu, ok)) {
@@ -547,7 +575,10 @@ __global__ void __launch_bounds__(TG / GPT * TX + 32)
             if (lane == 0) atomicExch(err, 1);
             break;
         }
-        consume_shot(i, st);
+        // most tiles need none of the rare parts of the epilogue (surface, accumulators, source,
+        // injection): decided per tile and shot, so that the common loop body stays lean
+        if (!rare_tile && !s_spec[i]) consume_shot(i, st, std::true_type());
+        else consume_shot(i, st, std::false_type());
         __syncwarp();
         if (lane == 0) mbar_arrive(smem_u32(&empty[st]));
     }
