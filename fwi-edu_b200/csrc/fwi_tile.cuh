@@ -316,6 +316,7 @@ __global__ void __launch_bounds__(TG / GPT * TX + 32)
     unsigned char *st_base = smem + Geo::ST_OFF;
     const bool producer = warp == NW && lane == 0;
     int issued = 0;  // shots whose copies the producer has issued
+    bool spec_here = false;
     if (producer) {
         // ---- barriers, then the coefficient tile and the first NST shots' copies at once: the
         // copies are in flight while the consumers compute the per-shot scalars
@@ -360,8 +361,11 @@ __global__ void __launch_bounds__(TG / GPT * TX + 32)
                            D.isz < Z0t + 4 * TG;
         const bool inj_t = kind == K_ADJ && it >= 1 && Z0t + 4 * TG > D.rz0 && Z0t <= D.rz1;
         s_spec[tid] = src_t || inj_t;
+        spec_here = s_spec[tid];
     }
-    __syncthreads();  // barriers and the per-shot scalars; no block-wide barrier follows
+    // barriers and the per-shot scalars; no block-wide barrier follows.  any_spec: some shot of
+    // the chunk has its source or receiver rows in this tile
+    const bool any_spec = __syncthreads_or(spec_here) != 0;
     grid_dep_wait();  // fields and accumulators: after the previous step (the producer waited already)
 
     if (warp == NW) {
@@ -568,20 +572,25 @@ __global__ void __launch_bounds__(TG / GPT * TX + 32)
             for (int f = 0; f < 6; ++f) cfh[f] = scf[f][k][zl];
         }
     }
-    for (int i = 0; i < n; ++i) {
-        const int st = i % NST;
-        bool ok = mbar_wait(smem_u32(&full[st]), (i / NST) & 1);
-        if (!__all_sync(0xffffffffu, ok)) {  // the warp gives up as one
-            if (lane == 0) atomicExch(err, 1);
-            break;
+    // the shots of the chunk in order; PLAIN: no shot needs the rare parts of the epilogue in
+    // this tile (surface, accumulators, source, injection), so the loop holds the store-only
+    // consumer alone and stays lean
+    auto walk = [&](auto plain) {
+        for (int i = 0; i < n; ++i) {
+            const int st = i % NST;
+            bool ok = mbar_wait(smem_u32(&full[st]), (i / NST) & 1);
+            if (!__all_sync(0xffffffffu, ok)) {  // the warp gives up as one
+                if (lane == 0) atomicExch(err, 1);
+                break;
+            }
+            if (decltype(plain)::value || (!rare_tile && !s_spec[i])) consume_shot(i, st, std::true_type());
+            else consume_shot(i, st, std::false_type());
+            __syncwarp();
+            if (lane == 0) mbar_arrive(smem_u32(&empty[st]));
         }
-        // most tiles need none of the rare parts of the epilogue (surface, accumulators, source,
-        // injection): decided per tile and shot, so that the common loop body stays lean
-        if (!rare_tile && !s_spec[i]) consume_shot(i, st, std::true_type());
-        else consume_shot(i, st, std::false_type());
-        __syncwarp();
-        if (lane == 0) mbar_arrive(smem_u32(&empty[st]));
-    }
+    };
+    if (!rare_tile && !any_spec) walk(std::true_type());
+    else walk(std::false_type());
 }
 
 }  // namespace fwi
