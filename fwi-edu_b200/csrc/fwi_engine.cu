@@ -783,11 +783,13 @@ static LaunchCfg pick_launch(int Nx, int nshot, bool batched, int math)
 typedef void (*TileFn)(const CUtensorMap, const CUtensorMap, const CUtensorMap, const ShotDesc *, const int4 *, int,
                        int, int, int, int *);
 
-template <int TX, int NST, int MATH, int GPT>
+template <int TX, int NST, int MATH, int GPT, int MINB>
 static TileFn tile_fn()
 {
     static bool ready = false;
-    TileFn f = k_tile<TX, NST, MATH, GPT>;
+    TileFn f;
+    if constexpr (MINB == 3) f = k_tile3<TX, NST, MATH>;
+    else f = k_tile<TX, NST, MATH, GPT>;
     if (!ready) {
         cudaFuncSetAttribute((const void *)f, cudaFuncAttributeMaxDynamicSharedMemorySize, TileGeom<TX>::smem(NST));
         cudaFuncSetAttribute((const void *)f, cudaFuncAttributePreferredSharedMemoryCarveout,
@@ -797,16 +799,22 @@ static TileFn tile_fn()
     return f;
 }
 
-template <int TX, int MATH, int GPT>
+template <int TX, int MATH, int GPT, int MINB>
 static TileFn tile_fn_nst(int nst)
 {
-    return nst == 2 ? tile_fn<TX, 2, MATH, GPT>() : nst == 4 ? tile_fn<TX, 4, MATH, GPT>() : tile_fn<TX, 3, MATH, GPT>();
+    return nst == 2   ? tile_fn<TX, 2, MATH, GPT, MINB>()
+           : nst == 4 ? tile_fn<TX, 4, MATH, GPT, MINB>()
+                      : tile_fn<TX, 3, MATH, GPT, MINB>();
 }
 
+// MINB 3 (coefficients from shared memory, three blocks per SM) exists for 16-column tiles with
+// one group per thread, the shape that register use limits to two blocks
 template <int TX, int MATH>
-static TileFn tile_fn_gpt(int nst, int gpt)
+static TileFn tile_fn_gpt(int nst, int gpt, int minb)
 {
-    return gpt == 2 ? tile_fn_nst<TX, MATH, 2>(nst) : tile_fn_nst<TX, MATH, 1>(nst);
+    if (gpt == 2) return tile_fn_nst<TX, MATH, 2, 1>(nst);
+    if (TX == 16 && minb == 3) return tile_fn_nst<TX, MATH, 1, TX == 16 ? 3 : 1>(nst);
+    return tile_fn_nst<TX, MATH, 1, 1>(nst);
 }
 
 // shots per block: split the group into equal chunks (at most 12 shots each, the measured
@@ -836,6 +844,7 @@ static int check_kernel_error(fwi_ctx *c);
 // ring (2..4 shots in flight) and shots per block (the chunk).
 struct TileCfg {
     int tx = 16, nst = 4, chunk = 1, gpt = 1;  // gpt: z-groups per consumer thread (1 or 2)
+    int minb = 1;                              // 3: the three-blocks-per-SM variant (tx 16, gpt 1)
 };
 
 static int launch_tiles(fwi_ctx *c, const Program *prog, int L0, int L1, int shot_base, int nshot, const ShotRun *r0,
@@ -844,8 +853,9 @@ static int launch_tiles(fwi_ctx *c, const Program *prog, int L0, int L1, int sho
     const Plan *p = r0->plan;
     const int zt = (p->G + TG - 1) / TG;
     const int tx = cfg.tx, nst = cfg.nst, chunk = cfg.chunk, gpt = cfg.gpt, nl = TG / gpt;
-    TileFn fn = tx == 16 ? (c->math ? tile_fn_gpt<16, 1>(nst, gpt) : tile_fn_gpt<16, 0>(nst, gpt))
-                         : (c->math ? tile_fn_gpt<8, 1>(nst, gpt) : tile_fn_gpt<8, 0>(nst, gpt));
+    const int minb = cfg.minb;
+    TileFn fn = tx == 16 ? (c->math ? tile_fn_gpt<16, 1>(nst, gpt, minb) : tile_fn_gpt<16, 0>(nst, gpt, minb))
+                         : (c->math ? tile_fn_gpt<8, 1>(nst, gpt, minb) : tile_fn_gpt<8, 0>(nst, gpt, minb));
     const int smem = tx == 16 ? TileGeom<16>::smem(nst) : TileGeom<8>::smem(nst);
     const int ntx = (p->Nx + tx - 1) / tx, nchunks = (nshot + chunk - 1) / chunk;
     dim3 grid(ntx + 1, 2 * nchunks, zt);
@@ -903,6 +913,7 @@ static TileCfg tile_config(fwi_ctx *c, const Plan *p, int nshot, bool batched)
     if (const char *e = getenv("FWI_NST")) cfg.nst = std::min(4, std::max(2, atoi(e)));
     if (const char *e = getenv("FWI_CHUNK")) cfg.chunk = std::min(TILE_CH_MAX, std::max(1, atoi(e)));
     if (const char *e = getenv("FWI_GPT")) cfg.gpt = atoi(e) == 2 ? 2 : 1;
+    if (const char *e = getenv("FWI_OCC")) cfg.minb = atoi(e) == 3 ? 3 : 1;
     cfg.chunk = std::min(cfg.chunk, std::max(1, nshot));
     c->last_tx = cfg.tx;
     c->last_nst = cfg.nst;
@@ -932,7 +943,9 @@ static int autotune(fwi_ctx *c, int shot_base, int nshot, const ShotRun *r0, boo
     std::vector<TileCfg> cands;
     for (int gpt : {1, 2})
         for (int tx : {16, 8})
+            for (int minb : {1, 3})
             for (int nst : {2, 3, 4}) {
+                if (minb == 3 && (tx != 16 || gpt != 1)) continue;
                 std::set<int> chunks;
                 for (int cap : {4, 8, 12, 16, 24}) {
                     const int nch = (nshot + cap - 1) / cap;
@@ -945,6 +958,7 @@ static int autotune(fwi_ctx *c, int shot_base, int nshot, const ShotRun *r0, boo
                     t.nst = nst;
                     t.chunk = ch;
                     t.gpt = gpt;
+                    t.minb = minb;
                     cands.push_back(t);
                 }
             }
@@ -1414,7 +1428,8 @@ static int run_program(fwi_ctx *c, const std::string &key, const Program *prog, 
 {
     const char *ke = getenv("FWI_KERNEL");
     const bool tile_kernel = !(ke && strcmp(ke, "step") == 0);
-    if (c->tune && tile_kernel && !getenv("FWI_TX") && !getenv("FWI_NST") && !getenv("FWI_CHUNK") && !getenv("FWI_GPT"))
+    if (c->tune && tile_kernel && !getenv("FWI_TX") && !getenv("FWI_NST") && !getenv("FWI_CHUNK") && !getenv("FWI_GPT") &&
+        !getenv("FWI_OCC"))
         TRY(autotune(c, shot_base, nshot, r0, batched));
     if (!batched) return launch_steps(c, prog, shot_base, nshot, r0, false);
     if (!c->use_graphs) return launch_steps(c, prog, shot_base, nshot, r0, true);

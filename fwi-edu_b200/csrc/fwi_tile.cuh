@@ -264,11 +264,14 @@ struct TileGeom {
 // Tensor maps: tm_p1 / tm_p0 describe the group's frame pool {ld, Nx, nfr, nshot} (z
 // contiguous; shot s of the group at index s - shot_base) with boxes {ZP, XP, 1, 1} and
 // {ZC, TX, 1, 1}; tm_cf the six coefficient planes {ld, Nx, 6} with box {ZC, TX, 6}.
-template <int TX, int NST, int MATH, int GPT>
-__global__ void __launch_bounds__(TG / GPT * TX + 32)
-    k_tile(const __grid_constant__ CUtensorMap tm_p1, const __grid_constant__ CUtensorMap tm_p0,
-           const __grid_constant__ CUtensorMap tm_cf, const ShotDesc *__restrict__ shots, const int4 *__restrict__ prog,
-           int L, int shot_base, int nshot, int chunk, int *err)
+// MINB: blocks per SM the kernel is compiled for.  1 (k_tile, no minimum): with one group per
+// thread the six coefficient float4s stay in registers for the chunk; 3 (k_tile3): they are read
+// from shared memory per shot instead, which fits three blocks per SM (more warps to hide
+// latency, at six more shared loads per group and shot).
+template <int TX, int NST, int MATH, int GPT, int MINB>
+__device__ __forceinline__ void tile_body(const CUtensorMap &tm_p1, const CUtensorMap &tm_p0, const CUtensorMap &tm_cf,
+                                          const ShotDesc *__restrict__ shots, const int4 *__restrict__ prog, int L,
+                                          int shot_base, int nshot, int chunk, int *err)
 {
     using Geo = TileGeom<TX>;
     constexpr int NL = TG / GPT;  // consumer lanes per column
@@ -427,7 +430,8 @@ __global__ void __launch_bounds__(TG / GPT * TX + 32)
     K.idzz = pk(A.invdzdz, A.invdzdz);
     const float4 zero4 = make_float4(0.f, 0.f, 0.f, 0.f);
     const float4(*scf)[TX][TG] = reinterpret_cast<const float4(*)[TX][TG]>(smem);
-    float4 cfh[6];  // one group per thread: its coefficients stay in registers for the chunk
+    constexpr bool CF_REG = GPT == 1 && MINB < 3;
+    float4 cfh[6];  // CF_REG: the thread's coefficients stay in registers for the chunk
 
     // group gl of the tile for shot i: stencil from the stage, fused epilogue, store;
     // lo / cq / hi are groups gl-1, gl, gl+1 of column x
@@ -444,7 +448,7 @@ __global__ void __launch_bounds__(TG / GPT * TX + 32)
             const unsigned xa = sb + (unsigned)(cx * (TG + 2) + cg) * 16u, cs = (TG + 2) * 16u;
             const float4 xn[6] = {lds4(xa - 3 * cs), lds4(xa - 2 * cs), lds4(xa - cs),
                                   lds4(xa + cs), lds4(xa + 2 * cs), lds4(xa + 3 * cs)};
-            if (GPT == 1) {
+            if (CF_REG) {
                 v = group2<MATH>(lo, cq, hi, xn, cfh, p0, K);
             } else {
                 const float4 cf[6] = {scf[0][k][gl], scf[1][k][gl], scf[2][k][gl],
@@ -567,7 +571,7 @@ __global__ void __launch_bounds__(TG / GPT * TX + 32)
             if (lane == 0) atomicExch(err, 1);
             return;
         }
-        if (GPT == 1) {
+        if (CF_REG) {
 #pragma unroll
             for (int f = 0; f < 6; ++f) cfh[f] = scf[f][k][zl];
         }
@@ -591,6 +595,28 @@ __global__ void __launch_bounds__(TG / GPT * TX + 32)
     };
     if (!rare_tile && !any_spec) walk(std::true_type());
     else walk(std::false_type());
+}
+
+// the step kernel; the tensor maps are kernel parameters in constant space (the body takes
+// their addresses)
+template <int TX, int NST, int MATH, int GPT>
+__global__ void __launch_bounds__(TG / GPT * TX + 32)
+    k_tile(const __grid_constant__ CUtensorMap tm_p1, const __grid_constant__ CUtensorMap tm_p0,
+           const __grid_constant__ CUtensorMap tm_cf, const ShotDesc *__restrict__ shots, const int4 *__restrict__ prog,
+           int L, int shot_base, int nshot, int chunk, int *err)
+{
+    tile_body<TX, NST, MATH, GPT, 1>(tm_p1, tm_p0, tm_cf, shots, prog, L, shot_base, nshot, chunk, err);
+}
+
+// the same step compiled for three blocks per SM, one group per thread, coefficients read from
+// shared memory per shot
+template <int TX, int NST, int MATH>
+__global__ void __launch_bounds__(TG * TX + 32, 3)
+    k_tile3(const __grid_constant__ CUtensorMap tm_p1, const __grid_constant__ CUtensorMap tm_p0,
+            const __grid_constant__ CUtensorMap tm_cf, const ShotDesc *__restrict__ shots, const int4 *__restrict__ prog,
+            int L, int shot_base, int nshot, int chunk, int *err)
+{
+    tile_body<TX, NST, MATH, 1, 3>(tm_p1, tm_p0, tm_cf, shots, prog, L, shot_base, nshot, chunk, err);
 }
 
 }  // namespace fwi

@@ -28,8 +28,11 @@ SHAPES = [
     {"FWI_GPT": "2"},
     {"FWI_TX": "8", "FWI_GPT": "2", "FWI_NST": "3", "FWI_CHUNK": "5"},
     {"FWI_TX": "16", "FWI_GPT": "2", "FWI_NST": "2", "FWI_CHUNK": "1"},
+    {"FWI_OCC": "3"},
+    {"FWI_OCC": "3", "FWI_NST": "3", "FWI_CHUNK": "8"},
+    {"FWI_OCC": "3", "FWI_NST": "2", "FWI_CHUNK": "1"},
 ]
-KEYS = ("FWI_TX", "FWI_NST", "FWI_CHUNK", "FWI_KERNEL", "FWI_MATH", "FWI_TUNE", "FWI_GPT")
+KEYS = ("FWI_TX", "FWI_NST", "FWI_CHUNK", "FWI_KERNEL", "FWI_MATH", "FWI_TUNE", "FWI_GPT", "FWI_OCC")
 
 
 def rel(a, b):
