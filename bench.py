@@ -378,6 +378,7 @@ def step_roofline(ctx, E, peaks):
     ctx.run(0, path=E.PATH_BATCHED)
     st = ctx.stats()
     per_launch_ms = st["ms"] / st["kernel_launches"]
+    shape = ctx.launch_shape()
     cells_per_launch = st["cell_updates"] / NT
     # algorithmic bytes per cell-update with S shots stepping together on one coefficient set:
     # p1 read + p0 read + p2 write (12 B) + 6 coefficient planes read once for the S shots (24 B / S)
@@ -396,7 +397,8 @@ def step_roofline(ctx, E, peaks):
             "kernel": "k_tile (batched forward, 60 shots per launch)",
             "launch_us": per_launch_ms * 1e3, "gcells_per_s": cells_per_launch / (per_launch_ms * 1e-3) / 1e9,
             "bytes_per_cell_update": bpc, "algorithmic_bytes_per_launch": bytes_per_launch,
-            "shots_sharing_coefficients": S, "peak_source": "fallback" if peaks.get("fallback") else "measured"}
+            "shots_sharing_coefficients": S, "peak_source": "fallback" if peaks.get("fallback") else "measured",
+            "launch_shape": shape}
 
 
 def step_case(nshot, nt):

@@ -140,7 +140,7 @@ struct fwi_ctx {
     bool use_graphs = true;  // capture the batched launch sequences as CUDA graphs
     bool pdl = true;         // consecutive steps as programmatic dependent launches
     bool tune = true;        // time the step kernel's launch shapes once per shape (autotune)
-    int last_tx = 0, last_nst = 0, last_chunk = 0, last_gpt = 0;  // the shape of the last launch
+    int last_tx = 0, last_nst = 0, last_chunk = 0, last_gpt = 0, last_minb = 0;  // the shape of the last launch
     int *d_err = nullptr;  // set by a step kernel whose tile copy did not complete
     std::map<void *, size_t> sizes;  // live device blocks of this context
     size_t peak = 0;
@@ -919,6 +919,7 @@ static TileCfg tile_config(fwi_ctx *c, const Plan *p, int nshot, bool batched)
     c->last_nst = cfg.nst;
     c->last_chunk = cfg.chunk;
     c->last_gpt = cfg.gpt;
+    c->last_minb = cfg.minb;
     return cfg;
 }
 
@@ -1750,6 +1751,14 @@ extern "C" int fwi_ctx_launch_shape(fwi_ctx *c, int *tile_columns, int *ring_dep
     if (tile_columns) *tile_columns = c->last_tx;
     if (ring_depth) *ring_depth = c->last_nst;
     if (shots_per_block) *shots_per_block = c->last_chunk;
+    return FWI_OK;
+}
+
+extern "C" int fwi_ctx_launch_variant(fwi_ctx *c, int *groups_per_thread, int *blocks_per_sm)
+{
+    if (!c) return fail(FWI_ERR_ARG, "ctx is NULL");
+    if (groups_per_thread) *groups_per_thread = c->last_gpt;
+    if (blocks_per_sm) *blocks_per_sm = c->last_minb;
     return FWI_OK;
 }
 

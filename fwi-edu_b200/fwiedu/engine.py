@@ -285,6 +285,14 @@ class Context:
         self._ar = ALLREDUCE_FN(_cb)  # keep the thunk alive as long as the context
         _check(self.L.fwi_ctx_set_allreduce(self.h, self._ar, None))
 
+    def launch_shape(self):
+        """Shape of the last step launch (fwi_ctx_launch_shape, fwi_ctx_launch_variant)."""
+        v = [C.c_int() for _ in range(5)]
+        _check(self.L.fwi_ctx_launch_shape(self.h, C.byref(v[0]), C.byref(v[1]), C.byref(v[2])))
+        _check(self.L.fwi_ctx_launch_variant(self.h, C.byref(v[3]), C.byref(v[4])))
+        keys = ("tile_columns", "ring_depth", "shots_per_block", "groups_per_thread", "blocks_per_sm")
+        return {k: x.value for k, x in zip(keys, v)}
+
     def stats(self):
         s = FwiStats()
         _check(self.L.fwi_ctx_stats(self.h, C.byref(s)))

@@ -205,6 +205,10 @@ FWI_API int fwi_ctx_stats(fwi_ctx *ctx, fwi_stats *out);
  * a built-in heuristic.  fwi_ctx_launch_shape reports the shape of the last launch. */
 FWI_API int fwi_ctx_set_autotune(fwi_ctx *ctx, int on);
 FWI_API int fwi_ctx_launch_shape(fwi_ctx *ctx, int *tile_columns, int *ring_depth, int *shots_per_block);
+/* the rest of the last launch's shape: z-groups per consumer thread (1 or 2) and the blocks per SM
+ * the step kernel was compiled for (1: no minimum, coefficients in registers; 3: coefficients
+ * read from shared memory).  No counterpart in the reference. */
+FWI_API int fwi_ctx_launch_variant(fwi_ctx *ctx, int *groups_per_thread, int *blocks_per_sm);
 
 /* CUDA graphs on the batched path (default on; FWI_GRAPH=0 in the environment turns them off):
  * off, every step is launched directly -- cheaper for a launch sequence run only once. */
