@@ -365,6 +365,51 @@ def serving(E, M, nreq, rate, seed=0, max_active=4):
             "peak_active": rep["peak_active"], "peak_admitted_bytes": rep["peak_bytes"], "budget_bytes": rep["budget"]}
 
 
+# uneven-size gradient batch: (shots, nz, nx, d, dt, nt, Ricker peak)
+UNEVEN = [(128, 221, 601, 12.5, 0.001, 4001, 10.0), (64, 401, 1201, 10.0, 0.0008, 5001, 12.0),
+          (32, 301, 2001, 10.0, 0.0008, 6001, 10.0)]
+
+
+def uneven_batch():
+    """Gradient passes over three surveys of different grids and trace lengths (128 shots on
+    221x601, 64 on 401x1201, 32 on 301x2001), each model generated per seed as the others, as
+    three gradient requests to the serving loop: all submitted at once (concurrent on the GPU) and
+    one after another.  A first, untimed pass fills the autotuner's cache.  Observed data are
+    zero traces: the work of a gradient does not depend on their values."""
+    from fwiedu import engine as E
+    from fwiedu import models as M
+    reqs = []
+    for k, (ns, nz, nx, d, dt, nt, f) in enumerate(UNEVEN):
+        vp = M.layered_model(nz, nx, seed=300 + k, water_rows=WATER)
+        rho = M.gardner(vp, water_rows=WATER)
+        src = M.ricker(nt, dt, f, 1.5 / f)
+        sv = M.line_survey(nz, nx, d, d, dt, nt, ns, src, spacing_cells=(nx - 1) // ns, first_cell=0)
+        shots = M.survey_shots(sv)
+        zero = np.zeros((len(shots[0].igx), shots[0].ns), np.float32)
+        reqs.append(E.request(E.REQ_GRADIENT, vp=vp, rho=rho, dx=d, dz=d, dt=dt, nt=nt, pml=PML, fs=FS, shots=shots,
+                              obs=[zero] * ns))
+
+    def once(active):
+        srv = E.Server(0, 0, max_active=active)
+        t0 = time.perf_counter()
+        ids = [srv.submit(r, h) for r, h in reqs]
+        infos = [srv.wait(i) for i in ids]
+        wall = time.perf_counter() - t0
+        rep = srv.report()
+        srv.close()
+        return {"wall_s": wall, "failed": rep["failed"], "shot_gradients_per_s": sum(u[0] for u in UNEVEN) / wall,
+                "gcells_per_s": rep["cell_updates"] / wall / 1e9, "peak_active": rep["peak_active"],
+                "peak_admitted_bytes": rep["peak_bytes"],
+                "service_ms": [round(x["run_ms"], 1) for x in infos], "status": [x["status"] for x in infos]}
+
+    once(1)  # warm-up: autotuned launch shapes, device memory pool
+    seq = once(1)
+    conc = once(3)
+    print(json.dumps({"workload": "uneven-size gradient batch: 128 shots 221x601 nt 4001, 64 shots 401x1201 nt 5001, "
+                                  "32 shots 301x2001 nt 6001 (gradient passes through the serving loop)",
+                      "unit": "shot-gradients/s", "concurrent": conc, "one_at_a_time": seq}), flush=True)
+
+
 # ------------------------------------------------------------------ roofline
 TRAFFIC = os.path.join(ROOT, "profiles", "k_tile_forward_60shots_traffic.json")
 
@@ -429,12 +474,16 @@ def main():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--serve-requests", type=int, default=40, help="requests of the serving measurement (0: skip)")
     ap.add_argument("--serve-rate", type=float, default=20.0, help="Poisson arrival rate of the serving measurement")
+    ap.add_argument("--uneven-batch", action="store_true",
+                    help="gradient passes over three surveys of different grids through the serving loop (own line)")
     ap.add_argument("--step-case", nargs=2, type=int, metavar=("SHOTS", "NT"),
                     help="profiling case: one batched forward of SHOTS shots of the survey for NT steps, no JSON line")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
     if args.step_case:
         return step_case(*args.step_case)
+    if args.uneven_batch:
+        return uneven_batch()
     if args.impl == "reference":
         return run_reference_arm(args)
 
