@@ -410,6 +410,39 @@ def uneven_batch():
                       "unit": "shot-gradients/s", "concurrent": conc, "one_at_a_time": seq}), flush=True)
 
 
+def large_survey(nshot=100):
+    """One gradient over the precision-study grid (1201 x 4001 at 5 m, 8001 steps of 0.4 ms, 20 Hz
+    Ricker, 100 shots, 4001 receivers each): about 4 GB of checkpoint frames per shot, far more
+    than the device holds for all shots, so the batched path runs the shots in waves.  Observed
+    data are zero traces (the work does not depend on their values)."""
+    from fwiedu import engine as E
+    from fwiedu import models as M
+    nz, nx, d, dt, nt = 1201, 4001, 5.0, 0.0004, 8001
+    vp = M.layered_model(nz, nx, seed=7, water_rows=WATER)
+    rho = M.gardner(vp, water_rows=WATER)
+    src = M.ricker(nt, dt, 20.0, 0.075)
+    sv = M.line_survey(nz, nx, d, d, dt, nt, nshot, src, spacing_cells=(nx - 1) // nshot, first_cell=0)
+    shots = M.survey_shots(sv)
+    zero = np.zeros((len(shots[0].igx), shots[0].ns), np.float32)
+    ctx = E.Context(0)
+    try:
+        ctx.set_model(vp, rho, d, d, dt, nt, PML, FS)
+        ctx.set_shots(shots)
+        ctx.set_observed([zero] * nshot)
+        t0 = time.perf_counter()
+        ctx.run(1, 20.0, 2, 1, E.PATH_BATCHED)
+        wall = time.perf_counter() - t0
+        st = ctx.stats()
+        g = ctx.gradient()
+    finally:
+        ctx.close()
+    print(json.dumps({"workload": f"gradient, {nshot} shots on 1201x4001 (5 m), nt 8001, 4001 receivers",
+                      "unit": "shot-gradients/s", "value": nshot / (st["ms"] / 1e3), "device_s": st["ms"] / 1e3,
+                      "wall_s": wall, "gcells_per_s": st["cell_updates"] / st["ms"] / 1e6,
+                      "device_bytes_held": st["device_bytes"], "kernel_launches": st["kernel_launches"],
+                      "gradient_finite": bool(np.isfinite(g).all())}), flush=True)
+
+
 # ------------------------------------------------------------------ roofline
 TRAFFIC = os.path.join(ROOT, "profiles", "k_tile_forward_60shots_traffic.json")
 
@@ -474,6 +507,8 @@ def main():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--serve-requests", type=int, default=40, help="requests of the serving measurement (0: skip)")
     ap.add_argument("--serve-rate", type=float, default=20.0, help="Poisson arrival rate of the serving measurement")
+    ap.add_argument("--large-survey", action="store_true",
+                    help="one gradient over 100 shots on the 1201 x 4001 grid, run in waves (own line)")
     ap.add_argument("--uneven-batch", action="store_true",
                     help="gradient passes over three surveys of different grids through the serving loop (own line)")
     ap.add_argument("--step-case", nargs=2, type=int, metavar=("SHOTS", "NT"),
@@ -484,6 +519,8 @@ def main():
         return step_case(*args.step_case)
     if args.uneven_batch:
         return uneven_batch()
+    if args.large_survey:
+        return large_survey()
     if args.impl == "reference":
         return run_reference_arm(args)
 
