@@ -942,26 +942,26 @@ static int autotune(fwi_ctx *c, int shot_base, int nshot, const ShotRun *r0, boo
     Program *prog;
     TRY(get_program(c, "tune/" + std::to_string(steps), items, &prog));
     std::vector<TileCfg> cands;
+    std::set<int> chunks;  // even splits of the shots into blocks of at most 4 .. 24
+    for (int cap : {4, 8, 12, 16, 24}) {
+        const int nch = (nshot + cap - 1) / cap;
+        chunks.insert((nshot + nch - 1) / nch);
+    }
     for (int gpt : {1, 2})
         for (int tx : {16, 8})
-            for (int minb : {1, 3})
-            for (int nst : {2, 3, 4}) {
-                if (minb == 3 && (tx != 16 || gpt != 1)) continue;
-                std::set<int> chunks;
-                for (int cap : {4, 8, 12, 16, 24}) {
-                    const int nch = (nshot + cap - 1) / cap;
-                    chunks.insert((nshot + nch - 1) / nch);
-                }
-                for (int ch : chunks) {
-                    if (nshot == 1 && nst != 2) continue;  // one shot: the ring depth does not matter
-                    TileCfg t;
-                    t.tx = tx;
-                    t.nst = nst;
-                    t.chunk = ch;
-                    t.gpt = gpt;
-                    t.minb = minb;
-                    cands.push_back(t);
-                }
+            for (int minb : {1, 3}) {
+                if (minb == 3 && (tx != 16 || gpt != 1)) continue;  // k_tile3 exists for this shape only
+                for (int nst : {2, 3, 4})
+                    for (int ch : chunks) {
+                        if (nshot == 1 && nst != 2) continue;  // one shot: the ring depth does not matter
+                        TileCfg t;
+                        t.tx = tx;
+                        t.nst = nst;
+                        t.chunk = ch;
+                        t.gpt = gpt;
+                        t.minb = minb;
+                        cands.push_back(t);
+                    }
             }
     const long long l0 = c->launches;
     float best_ms = 1e30f;
