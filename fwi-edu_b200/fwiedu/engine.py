@@ -95,6 +95,8 @@ def lib():
             L.fwi_ctx_traces_device.restype = C.c_void_p
             L.fwi_ctx_gradient_device.restype = C.c_void_p
             L.calculate_memory_cost_checkpoint.restype = C.c_float
+            L.fwi_request_bytes.restype = C.c_size_t
+            L.fwi_estimate_bytes.restype = C.c_size_t
             _lib = L
     return _lib
 
@@ -374,8 +376,6 @@ class Server:
 
     def __init__(self, device=0, budget_bytes=0, max_active=4):
         self.L = lib()
-        self.L.fwi_request_bytes.restype = C.c_size_t
-        self.L.fwi_estimate_bytes.restype = C.c_size_t
         self.h = C.c_void_p()
         _check(self.L.fwi_server_create(C.byref(self.h), device, C.c_size_t(budget_bytes), max_active))
         self.pending = {}
@@ -419,7 +419,6 @@ class Server:
 def estimate_bytes(shots, nz, nx, nt, pml, problem, filt=2):
     """fwi_estimate_bytes: device bytes one context needs for the run (host-side, no GPU)."""
     L = lib()
-    L.fwi_estimate_bytes.restype = C.c_size_t
     keep = []
     arr = _shot_array(shots, keep)
     return int(L.fwi_estimate_bytes(arr, len(shots), nz, nx, nt, pml, problem, filt))
