@@ -198,11 +198,13 @@ typedef struct {
 } fwi_stats;
 FWI_API int fwi_ctx_stats(fwi_ctx *ctx, fwi_stats *out);
 
-/* The step kernel's launch shape (tile width 8/16 columns, shared-memory ring depth 2..4 shots,
- * shots per block) is picked by an autotuner: the first run of a launch shape (padded grid,
- * shots per launch, arithmetic, path) times the candidates on the run's own scratch frames and
- * keeps the fastest for the process.  Off (or FWI_TUNE=0; or FWI_TX / FWI_NST / FWI_CHUNK set):
- * a built-in heuristic.  fwi_ctx_launch_shape reports the shape of the last launch. */
+/* The step kernel's launch shape (tile width 8/16 columns, z-groups per thread, blocks per SM it
+ * is compiled for, shared-memory ring depth 2..4 shots, shots per block) is picked by an
+ * autotuner: the first run of a launch shape (padded grid, shots per launch, arithmetic, path)
+ * times the candidates on the run's own scratch frames and keeps the fastest for the process.
+ * Off (or FWI_TUNE=0; or any of FWI_TX / FWI_NST / FWI_CHUNK / FWI_GPT / FWI_OCC set): a built-in
+ * heuristic with those overrides.  fwi_ctx_launch_shape and fwi_ctx_launch_variant report the
+ * shape of the last launch. */
 FWI_API int fwi_ctx_set_autotune(fwi_ctx *ctx, int on);
 FWI_API int fwi_ctx_launch_shape(fwi_ctx *ctx, int *tile_columns, int *ring_depth, int *shots_per_block);
 /* the rest of the last launch's shape: z-groups per consumer thread (1 or 2) and the blocks per SM
