@@ -97,10 +97,11 @@ __device__ __forceinline__ u64 cell2(u64 zm3, u64 zm2, u64 zm1, u64 z0, u64 zp1,
             const float2 x = upk(a), y = upk(b);
             return pk(__fmul_rn(x.x, y.x), __fmul_rn(x.y, y.y));
         };
-        const u64 dpdz = mul(add2(add2(mul(k.C1, sub2(zp1, zm1)), mul(k.C2, sub2(zp2, zm2))), mul(k.C3, sub2(zp3, zm3))),
-                             k.idz);
-        const u64 dpdx = mul(add2(add2(mul(k.C1, sub2(xp1, xm1)), mul(k.C2, sub2(xp2, xm2))), mul(k.C3, sub2(xp3, xm3))),
-                             k.idx);
+        // dpdz and dpdx feed multiplies only: a packed multiply there cannot be fused into an add
+        const u64 dpdz =
+            mul2(add2(add2(mul(k.C1, sub2(zp1, zm1)), mul(k.C2, sub2(zp2, zm2))), mul(k.C3, sub2(zp3, zm3))), k.idz);
+        const u64 dpdx =
+            mul2(add2(add2(mul(k.C1, sub2(xp1, xm1)), mul(k.C2, sub2(xp2, xm2))), mul(k.C3, sub2(xp3, xm3))), k.idx);
         const u64 d0 = mul(k.D0, z0);
         const u64 dzz =
             mul(add2(add2(add2(d0, mul(k.D1, add2(zp1, zm1))), mul(k.D2, add2(zp2, zm2))), mul(k.D3, add2(zp3, zm3))),
