@@ -159,3 +159,23 @@ def test_autotuned_shape_is_bit_identical_and_cached():
     assert all(np.array_equal(a, b) for a, b in zip(pre, ref_pre))
     assert all(np.array_equal(a, b) for a, b in zip(adj, ref_adj))
     assert np.array_equal(grad, ref_grad)
+
+
+def test_many_receivers_match_cp_async_kernel():
+    """More receivers than one pass of the sampling blocks covers (a shallow model has one tile
+    of rows, so 288 gathers per pass against 1500 receivers): every trace sample is the cp.async
+    kernel's, bit for bit, in both compiled variants and the narrow tiles."""
+    nz, nx, nt = 30, 1500, 120
+    vp = M.layered_model(nz, nx, seed=11, water_rows=4)
+    rho = M.gardner(vp, water_rows=4)
+    src = M.ricker(nt, 0.001, 15.0, 0.06)
+    sv = M.line_survey(nz, nx, 10.0, 10.0, 0.001, nt, 3, src, spacing_cells=400, first_cell=100)
+    shots = M.survey_shots(sv)
+    assert all(len(s.igx) == nx for s in shots)  # a receiver in every column
+    with env(FWI_KERNEL="step"):
+        ref, _ = run_case(vp, rho, 10.0, 0.001, nt, 10, 1, shots)
+    for shape in ({}, {"FWI_OCC": "3"}, {"FWI_TX": "8"}):
+        with env(**shape):
+            got, _ = run_case(vp, rho, 10.0, 0.001, nt, 10, 1, shots)
+        for i, (a, b) in enumerate(zip(got, ref)):
+            assert np.array_equal(a, b), (shape, i)
