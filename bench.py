@@ -405,9 +405,13 @@ def uneven_batch():
     once(1)  # warm-up: autotuned launch shapes, device memory pool
     seq = once(1)
     conc = once(3)
-    print(json.dumps({"workload": "uneven-size gradient batch: 128 shots 221x601 nt 4001, 64 shots 401x1201 nt 5001, "
-                                  "32 shots 301x2001 nt 6001 (gradient passes through the serving loop)",
-                      "unit": "shot-gradients/s", "concurrent": conc, "one_at_a_time": seq}), flush=True)
+    return {"workload": "uneven-size gradient batch: 128 shots 221x601 nt 4001, 64 shots 401x1201 nt 5001, "
+                        "32 shots 301x2001 nt 6001 (gradient passes through the serving loop)",
+            "unit": "shot-gradients/s", "value": conc["shot_gradients_per_s"], "concurrent": conc,
+            "one_at_a_time": seq}
+
+
+LARGE_SAMPLE = 24  # shots of the large-grid survey in the default bench line (one wave)
 
 
 def large_survey(nshot=100):
@@ -436,11 +440,83 @@ def large_survey(nshot=100):
         g = ctx.gradient()
     finally:
         ctx.close()
-    print(json.dumps({"workload": f"gradient, {nshot} shots on 1201x4001 (5 m), nt 8001, 4001 receivers",
-                      "unit": "shot-gradients/s", "value": nshot / (st["ms"] / 1e3), "device_s": st["ms"] / 1e3,
-                      "wall_s": wall, "gcells_per_s": st["cell_updates"] / st["ms"] / 1e6,
-                      "device_bytes_held": st["device_bytes"], "kernel_launches": st["kernel_launches"],
-                      "gradient_finite": bool(np.isfinite(g).all())}), flush=True)
+    return {"workload": f"gradient, {nshot} shots on 1201x4001 (5 m), nt 8001, 4001 receivers",
+            "unit": "shot-gradients/s", "value": nshot / (st["ms"] / 1e3), "device_s": st["ms"] / 1e3,
+            "wall_s": wall, "gcells_per_s": st["cell_updates"] / st["ms"] / 1e6,
+            "device_bytes_held": st["device_bytes"], "kernel_launches": st["kernel_launches"],
+            "gradient_finite": bool(np.isfinite(g).all())}
+
+
+# ------------------------------------------------------------------ plain path
+def l2_peak_gbs(local=0):
+    """L2 bandwidth of this GPU, measured here: an L2-resident STREAM-style copy (two 16 MiB
+    buffers swept 200 times inside one launch, fwi_l2_copy_probe).  No driver-measured L2 figure
+    exists; this is the denominator of the plain path's roofline."""
+    import torch
+    from fwiedu import engine as E
+    n = 16 << 20
+    a = torch.zeros(n // 4, device=f"cuda:{local}")
+    b = torch.zeros_like(a)
+    ms = C.c_float()
+    passes = 200
+    best = 0.0
+    for _ in range(3):
+        rc = E.lib().fwi_l2_copy_probe(C.c_void_p(a.data_ptr()), C.c_void_p(b.data_ptr()), C.c_longlong(n), passes,
+                                       None, C.byref(ms))
+        assert rc == 0
+        best = max(best, 2.0 * n * passes / (ms.value * 1e-3) / 1e9)
+    return best
+
+
+def plain_path(E, local, vp, rho, vp0, rho0, shots, obs, reps=2):
+    """The plain path (one shot per launch, shots one after another, as propagation.c:857 and
+    :895 loop over shots) on a 2-shot sample of the survey: a gradient iteration's engine work
+    (problem 1 then problem 2) and forward modeling (problem 0).  One untimed run of each first
+    (the autotuner times the one-shot launch shapes then), then `reps` timed runs; device time
+    from the engine's CUDA events.  Its step kernel works on one shot's 6.6 MB state, which stays
+    in L2: its roofline is the L2 copy bandwidth measured here."""
+    idx = [0, len(shots) // 2]
+    sh = [shots[i] for i in idx]
+    ob = [obs[i] for i in idx]
+    ctx = E.Context(local)
+    try:
+        ctx.set_model(vp0, rho0, DX, DX, DT, NT, PML, FS)
+        ctx.set_shots(sh)
+        ctx.set_observed(ob)
+        ms = cells = 0.0
+        for r in range(reps + 1):
+            ctx.run(1, ITER["freq"], ITER["filter"], 1, E.PATH_PLAIN)
+            a = ctx.stats()
+            ctx.run(2, ITER["freq"], ITER["filter"], 1, E.PATH_PLAIN)
+            b = ctx.stats()
+            if r:  # the first run is the warm-up
+                ms += a["ms"] + b["ms"]
+                cells += a["cell_updates"] + b["cell_updates"]
+        sgps = len(sh) * reps / (ms / 1e3)
+        gcells = cells / (ms * 1e6)
+        ctx.set_model(vp, rho, DX, DX, DT, NT, PML, FS)
+        fms = fcells = 0.0
+        flaunch = 0
+        for r in range(reps + 1):
+            ctx.run(0, path=E.PATH_PLAIN)
+            st = ctx.stats()
+            if r:
+                fms += st["ms"]
+                fcells += st["cell_updates"]
+                flaunch += st["kernel_launches"]
+    finally:
+        ctx.close()
+    l2 = l2_peak_gbs(local)
+    # one step launch of one shot: 12 B of fields + 24 B of its own coefficient planes per cell
+    bpc = 36.0
+    achieved = fcells * bpc / (fms * 1e-3) / 1e9
+    return {"shot_gradients_per_s": sgps, "gcells_per_s": gcells,
+            "forward_shots_per_s": len(sh) * reps / (fms / 1e3), "forward_gcells_per_s": fcells / (fms * 1e6),
+            "roofline": {"bound": "l2", "achieved": achieved, "peak": l2, "unit": "GB/s", "frac": achieved / l2,
+                         "bytes_per_cell_update": bpc, "launch_us": fms * 1e3 / max(flaunch, 1),
+                         "peak_source": "measured in this run: L2-resident copy, fwi_l2_copy_probe"},
+            "sample": f"shots {idx} of the survey, {reps} timed runs after one untimed (autotuner) run",
+            "note": "one shot per launch; gradient figure = problem 1 + problem 2 (the iteration's engine work)"}
 
 
 # ------------------------------------------------------------------ roofline
@@ -505,6 +581,7 @@ def main():
     ap.add_argument("--impl", default="mine", choices=["mine", "reference"])
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline sample")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-extra", action="store_true", help="skip the uneven-batch and large-grid sub-measurements")
     ap.add_argument("--serve-requests", type=int, default=40, help="requests of the serving measurement (0: skip)")
     ap.add_argument("--serve-rate", type=float, default=20.0, help="Poisson arrival rate of the serving measurement")
     ap.add_argument("--large-survey", action="store_true",
@@ -518,9 +595,9 @@ def main():
     if args.step_case:
         return step_case(*args.step_case)
     if args.uneven_batch:
-        return uneven_batch()
+        return print(json.dumps(uneven_batch()), flush=True)
     if args.large_survey:
-        return large_survey()
+        return print(json.dumps(large_survey()), flush=True)
     if args.impl == "reference":
         return run_reference_arm(args)
 
@@ -588,18 +665,8 @@ def main():
         dev_s = float(t.item())
     value = NSHOT * world * args.steps / dev_s
 
-    # plain path: one shot per launch, on a 2-shot subset of the same survey
-    plain_ctx = E.Context(local)
-    plain_ctx.set_model(vp0, rho0, DX, DX, DT, NT, PML, FS)
-    plain_ctx.set_shots(shots[:2])
-    plain_ctx.set_observed(obs[:2])
-    plain_ctx.run(1, ITER["freq"], ITER["filter"], 1, E.PATH_PLAIN)
-    pst = plain_ctx.stats()
-    plain_ctx.run(2, ITER["freq"], ITER["filter"], 1, E.PATH_PLAIN)
-    pst2 = plain_ctx.stats()
-    plain_sgps = 2 / ((pst["ms"] + pst2["ms"]) / 1e3)
-    plain_gcells = (pst["cell_updates"] + pst2["cell_updates"]) / ((pst["ms"] + pst2["ms"]) * 1e6)
-    plain_ctx.close()
+    plain = plain_path(E, local, vp, rho, vp0, rho0, shots, obs)
+    plain_sgps = plain["shot_gradients_per_s"]
 
     e2e = None
     if not args.no_e2e and sharded:
@@ -639,6 +706,15 @@ def main():
         from fwiedu import models as M
         serve = serving(E, M, args.serve_requests, args.serve_rate)
 
+    uneven = large = None
+    if rank == 0 and world == 1 and not args.no_extra:
+        ctx.close()  # the sub-measurements need the device memory
+        ctx = None
+        uneven = uneven_batch()
+        large = large_survey(LARGE_SAMPLE)
+        large["sample"] = (f"{LARGE_SAMPLE} of the 100 shots of the 1201x4001 survey (one wave); "
+                           "python bench.py --large-survey runs all 100 in waves")
+
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
         try:
@@ -656,21 +732,26 @@ def main():
                            "shots": NSHOT * world, "receivers": NX, "checkpoints_per_shot": 89,
                            "shots_per_rank": NSHOT,
                            "shot_rule": rule, "path": "batched", "arithmetic": "bit-exact FP32 (no FMA contraction)",
-                           "l2": "working set ~10 GB per step, far above the 126 MB L2; no flush needed",
+                           "l2": ("inputs larger than L2, no flush: a timed iteration sweeps ~11 GB of frames "
+                                  "(60 shots x ~190 MB); one step launch reads ~103 MB and writes ~49 MB"),
                            "parallelism": (f"shots sharded over {world} ranks, one NCCL FP64 all-reduce of the "
                                            "gradient/Hessian stacks + scalar sums per iteration" if sharded
                                            else "1 rank")},
                 "gcells_per_s": cells / dev_s / 1e9,
                 "latency_ms": {"p50": lat_sorted[len(lat) // 2],
                                "p99": lat_sorted[min(len(lat) - 1, int(round(0.99 * (len(lat) - 1))))]},
-                "plain": {"shot_gradients_per_s": plain_sgps, "gcells_per_s": plain_gcells,
-                          "note": "one shot per launch, same iteration minus the host model update, 2 shots"},
+                "plain": plain,
                 "batched_over_plain": value / world / plain_sgps,
+                "batched_over_plain_note": ("the plain path is the same TMA step kernel launched per shot; its "
+                                            "one-shot launches already fill most of the GPU, so batching adds "
+                                            "occupancy and shared coefficient reads, not an order of magnitude"),
+                "uneven_batch": uneven, "large_survey": large,
                 "wall_s": wall, "gpu_launches": launches, "roofline": roof, "cpu_baseline": cpu, "e2e": e2e,
                 "serving": serve,
                 "clocks": clk.summary()}
         print(json.dumps(line), flush=True)
-    ctx.close()
+    if ctx is not None:
+        ctx.close()
     if dist:
         dist.barrier()
         dist.destroy_process_group()

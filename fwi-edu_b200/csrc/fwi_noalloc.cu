@@ -24,6 +24,7 @@
 #include <mutex>
 
 #include "../../include/fwi_b200.h"
+#include "fwi_smooth.cuh"
 
 #define FWI_NOALLOC_MAX_CELLS (1 << 22)  // nx * nz limit of fwi_smooth2d_noalloc
 #define FWI_NOALLOC_MAX_HALF 32          // largest smoothing half-width
@@ -34,27 +35,15 @@ static __device__ __align__(256) float g_smooth_scratch[FWI_NOALLOC_MAX_CELLS];
 
 struct Window {
     float w[2 * FWI_NOALLOC_MAX_HALF + 1];
+    __device__ float operator[](int k) const { return w[k]; }
 };
 
-// one cos^2 pass (smooth2D, common.c:927-1040): z direction when zdir, x otherwise;
-// FP64 accumulation over the window in index order, as the reference accumulates
+// one cos^2 pass (smooth2D, common.c:927-1040) with the weights passed by value: the
+// engine's smoothing pass (fwi_smooth.cuh), reading nothing but its arguments
 __global__ void k_smooth_pass(const float *__restrict__ in, float *__restrict__ out, int nx, int nz, int N, int zdir,
                               Window w)
 {
-    const long long n = (long long)nx * nz;
-    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
-        const int ix = (int)(i / nz), iz = (int)(i % nz);
-        const int j = zdir ? iz : ix, n1 = zdir ? nz : nx;
-        const int ws = j >= N ? 0 : N - j, ds = j >= N ? j - N : 0;
-        const int we = (n1 - 1 - j < N) ? 2 * N - (N - (n1 - 1 - j)) : 2 * N;
-        double a1 = 0.0, a2 = 0.0;
-        for (int k = ws, k2 = ds; k <= we; ++k, ++k2) {
-            const float v = zdir ? in[(long long)ix * nz + k2] : in[(long long)k2 * nz + iz];
-            a1 = __dadd_rn(a1, (double)__fmul_rn(w.w[k], v));
-            a2 = __dadd_rn(a2, (double)w.w[k]);
-        }
-        out[i] = (float)__ddiv_rn(a1, __dadd_rn(a2, (double)FLT_MIN));
-    }
+    fwi::smooth_pass(in, out, nx, nz, N, zdir, w);
 }
 
 Window weights(int N)
@@ -69,6 +58,9 @@ Window weights(int N)
 }
 
 // device address of the scratch array, resolved once per device with that device current
+// (on the first call made on that device).  The address belongs to the CUDA context of that
+// first call: a process that resets the device (cudaDeviceReset) and goes on calling this
+// entry point gets a stale address, so such a process must not use it after a reset.
 std::mutex g_mu;
 float *g_addr[64];
 bool g_ready[64];

@@ -22,7 +22,8 @@ import numpy as np
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 REF_DIR = os.path.join(HERE, "_ref")
-REFERENCE_ROOT = "/root/reference/FWILab2d/FWILab2dCLangV1.2.6"
+# the reference checkout (C implementation); FWI_REFERENCE_ROOT overrides the default location
+REFERENCE_ROOT = os.environ.get("FWI_REFERENCE_ROOT", "/root/reference/FWILab2d/FWILab2dCLangV1.2.6")
 
 _fp = C.POINTER(C.c_float)
 _ip = C.POINTER(C.c_int)
@@ -237,7 +238,7 @@ def build_ref():
     """Compile the unmodified reference sources against the shim (needs the reference checkout)."""
     if not os.path.isdir(REFERENCE_ROOT):
         return False
-    subprocess.run(["make", "-s", "-C", HERE, "ref", "-j8"], check=True)
+    subprocess.run(["make", "-s", "-C", HERE, "ref", "-j8", f"REFROOT={REFERENCE_ROOT}"], check=True)
     return True
 
 
