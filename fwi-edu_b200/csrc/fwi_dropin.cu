@@ -72,8 +72,6 @@ extern "C" int fwi_iso_acoustic2d_propagation(float **vp, float **rho, Record2D 
                                               float filter, int precondition, int problem, int iter, int verbose,
                                               Record2D *pre, float **grad)
 {
-    (void)iter;
-    (void)verbose;
     std::lock_guard<std::mutex> lk(g_mu);
     if (!vp || !rho || !obs || !pre || Nshot <= 0) return FWI_ERR_ARG;
     if (problem == 1 && !grad) return FWI_ERR_ARG;
@@ -101,23 +99,27 @@ extern "C" int fwi_iso_acoustic2d_propagation(float **vp, float **rho, Record2D 
         g_di.dx = dx; g_di.dz = dz; g_di.dt = dt;
     }
     if (reshot || !same_shots(obs, Nshot, nt)) {
+        // the new geometry is built aside and becomes the cached one only once the context took it
+        g_di.shots.clear();
         std::vector<fwi_shot> sh(Nshot);
-        g_di.src.assign(Nshot, {});
-        g_di.igx.assign(Nshot, {});
-        g_di.igz.assign(Nshot, {});
+        std::vector<std::vector<float>> src(Nshot);
+        std::vector<std::vector<int>> igx(Nshot), igz(Nshot);
         for (int i = 0; i < Nshot; i++) {
             const Record2D &r = obs[i];
-            if (!r.src || !r.igx || !r.igz) return FWI_ERR_ARG;
-            g_di.src[i].assign(r.src, r.src + nt);
-            g_di.igx[i].assign(r.igx, r.igx + r.ntr);
-            g_di.igz[i].assign(r.igz, r.igz + r.ntr);
+            if (!r.src || !r.igx || !r.igz || r.ntr < 0) return FWI_ERR_ARG;
+            src[i].assign(r.src, r.src + nt);
+            igx[i].assign(r.igx, r.igx + r.ntr);
+            igz[i].assign(r.igz, r.igz + r.ntr);
             fwi_shot &s = sh[i];
             s.shotID = r.shotID; s.isx = r.isx; s.isz = r.isz; s.ntr = r.ntr; s.ns = r.ns;
             s.sampleRate = r.sampleRate; s.ix_min = r.ix_min; s.ix_max = r.ix_max;
             s.dt = r.dt; s.dtr = r.dtr; s.fpeak = r.fpeak;
-            s.src = g_di.src[i].data(); s.igx = g_di.igx[i].data(); s.igz = g_di.igz[i].data();
+            s.src = src[i].data(); s.igx = igx[i].data(); s.igz = igz[i].data();
         }
         if ((rc = fwi_ctx_set_shots(c, sh.data(), Nshot)) != FWI_OK) return rc;
+        g_di.src.swap(src);  // the vectors' buffers move with them: sh's pointers stay valid
+        g_di.igx.swap(igx);
+        g_di.igz.swap(igz);
         g_di.shots = sh;
     }
     if (problem == 1 || problem == 2) {
@@ -128,6 +130,8 @@ extern "C" int fwi_iso_acoustic2d_propagation(float **vp, float **rho, Record2D 
         }
         if ((rc = fwi_ctx_set_observed(c, o.data())) != FWI_OK) return rc;
     }
+    // the reference's intermediate files (shotInterval / snapInterval from the environment)
+    if ((rc = fwi_ctx_set_verbose(c, verbose, iter, 0, 0, nullptr)) != FWI_OK) return rc;
     if ((rc = fwi_ctx_run(c, problem, freq, (int)filter, precondition, env_path())) != FWI_OK) return rc;
     for (int i = 0; i < Nshot; i++) {
         if (!pre[i].traces_p || !contiguous(pre[i].traces_p, pre[i].ns, pre[i].ntr)) return FWI_ERR_ARG;

@@ -14,7 +14,6 @@
 // group go into every launch and the whole launch sequence is captured once as
 // a CUDA graph and replayed; on the plain path shots run one after another, one
 // launch per step, as the reference's shot loop does (propagation.c:857, :895).
-#include <cublas_v2.h>
 #include <cuda.h>
 #include <cudaTypedefs.h>  // PFN_cuTensorMapEncodeTiled
 #include <cuda_runtime.h>
@@ -27,6 +26,7 @@
 #include <cstring>
 #include <cstdint>
 #include <deque>
+#include <functional>
 #include <tuple>
 #include <map>
 #include <memory>
@@ -42,6 +42,7 @@
 #include "fwi_step.cuh"
 #include "fwi_tile.cuh"
 #include "fwi_optim.cuh"
+#include "fwi_fft.cuh"
 
 using namespace fwi;
 
@@ -157,13 +158,21 @@ struct fwi_ctx {
         long long frame = 0;
     };
     std::map<int, Pool> pools;
-    // residual filters and trace interpolation: cuBLAS (pedantic FP32) and the operator matrices
-    cublasHandle_t blas = nullptr;
+    // residual filters and trace interpolation: FFT spectra and twiddles, keyed by filter and size
     std::map<std::string, std::pair<float *, size_t>> ops;
     float *d_fft_tmp = nullptr;
     size_t fft_tmp_bytes = 0;
     long long launches = 0;
     double last_obj = 0.0;
+    // verbose output (the reference's intermediate files), fwi_ctx_set_verbose
+    struct Dump {
+        int verbose = 0, iter = 0;
+        int shot_interval = 20;    // every shot_interval-th shot is written out
+        int snap_interval = 1000;  // snapshot time steps (verbose > 1)
+        std::string dir;           // "" = the working directory, as the reference writes
+        bool warned = false;
+    } dump;
+    bool snapping = false;  // the launches being issued belong to a pass that writes snapshots
 };
 
 // Device memory comes from the stream-ordered allocator on the context's stream: a context
@@ -248,7 +257,6 @@ extern "C" int fwi_ctx_destroy(fwi_ctx *c)
     // everything left in the allocator table belongs to this context
     for (auto &kv : c->sizes) cudaFreeAsync(kv.first, c->stream);
     c->sizes.clear();
-    if (c->blas) cublasDestroy(c->blas);
     cudaStreamSynchronize(c->stream);
     cudaEventDestroy(c->ev0); cudaEventDestroy(c->ev1);
     cudaStreamDestroy(c->stream);
@@ -589,6 +597,7 @@ static int prepare_run(fwi_ctx *c, ShotRun *r, int shot, bool gradient)
         }
     }
     d.hessian = 0;
+    d.snap = c->dump.verbose > 1 ? c->dump.snap_interval : 0;
     // per-step source terms in the reference's precision (propagation.c:558 double, :662 float)
     const float Ks = hc.K[(size_t)d.isx * d.ld + d.isz];
     std::vector<double> sd(nt);
@@ -838,6 +847,7 @@ static int pick_chunk(int tiles, int nshot, int resident)
 }
 
 static int check_kernel_error(fwi_ctx *c);
+static int snapshots_after(fwi_ctx *c, const Program *prog, int L, int shot_base, int nshot);
 
 // ---------------------------------------------------------------- tile configuration and autotuner
 // A launch shape of the step kernel: tile width (8 or 16 columns), depth of the shared-memory
@@ -880,6 +890,7 @@ static int launch_tiles(fwi_ctx *c, const Program *prog, int L0, int L1, int sho
         CK(cudaLaunchKernelEx(&lc, fn, m1, m0, mc, (const ShotDesc *)c->d_desc, (const int4 *)prog->d, L, shot_base,
                               nshot, chunk, c->d_err));
         c->launches++;
+        if (c->snapping) TRY(snapshots_after(c, prog, L, shot_base, nshot));
     }
     CK(cudaGetLastError());
     return FWI_OK;
@@ -1030,6 +1041,165 @@ static int check_kernel_error(fwi_ctx *c)
     return FWI_OK;
 }
 
+// ---------------------------------------------------------------- verbose output
+// With verbose > 0 the reference writes intermediate results as raw float32 files (write_bin,
+// dataio.c:277-302) into the working directory: per written-out shot of a gradient run the
+// predicted traces, the adjoint source and the raw shot gradient, and per gradient the stacked
+// gradient and preconditioner (propagation.c:917-944, 996-1005); with verbose > 1 also wavefield
+// snapshots every snap_interval steps (propagation.c:597-601, 717-723).  File names and contents
+// are the reference's.
+static int write_floats(fwi_ctx *c, const char *name, const float *h, size_t n)
+{
+    const std::string path = c->dump.dir.empty() ? std::string(name) : c->dump.dir + "/" + name;
+    FILE *fp = fopen(path.c_str(), "wb");
+    if (!fp) return fail(FWI_ERR_ARG, "verbose output: cannot open %s for writing", path.c_str());
+    const size_t w = fwrite(h, 4, n, fp);
+    const int e = fclose(fp);
+    if (w != n || e) return fail(FWI_ERR_ARG, "verbose output: short write to %s", path.c_str());
+    return FWI_OK;
+}
+
+// n device floats (stream-ordered after the work queued so far) into a file
+static int dump_device(fwi_ctx *c, const char *name, const float *dev, size_t n)
+{
+    std::vector<float> h(n);
+    CK(cudaMemcpyAsync(h.data(), dev, n * 4, cudaMemcpyDeviceToHost, c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+    return write_floats(c, name, h.data(), n);
+}
+
+// one padded field [Nx][ld] of a shot as the reference's [Nx][Nz] array
+static int dump_frame(fwi_ctx *c, const char *name, const ShotDesc &d, int fi)
+{
+    std::vector<float> h((size_t)d.Nx * d.Nz);
+    CK(cudaMemcpy2DAsync(h.data(), (size_t)d.Nz * 4, frame_ptr(d, fi), (size_t)d.ld * 4, (size_t)d.Nz * 4, d.Nx,
+                         cudaMemcpyDeviceToHost, c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+    return write_floats(c, name, h.data(), h.size());
+}
+
+// driver-level files of a gradient run for the shots of one group, written once their adjoint
+// sources exist: predicted traces (before the residual; the forward gathers are kept time-major
+// in traces_t), adjoint source ([ntr][ns] in d_pre) -- propagation.c:917-934
+static int dump_shot_traces(fwi_ctx *c, const std::vector<ShotRun *> &rs)
+{
+    if (c->dump.verbose < 1) return FWI_OK;
+    char name[256];
+    for (ShotRun *r : rs) {
+        if (r->shot % c->dump.shot_interval != 0) continue;
+        const fwi_shot &s = c->shots[r->shot].s;
+        const int ns = r->d.ns, ntr = r->d.ntr;
+        std::vector<float> t((size_t)ns * ntr), p((size_t)ns * ntr);
+        CK(cudaMemcpyAsync(t.data(), r->d.traces_t, t.size() * 4, cudaMemcpyDeviceToHost, c->stream));
+        CK(cudaStreamSynchronize(c->stream));
+        for (int k = 0; k < ns; k++)
+            for (int i = 0; i < ntr; i++) p[(size_t)i * ns + k] = t[(size_t)k * ntr + i];
+        snprintf(name, sizeof name, "predicted_iter%03d_shot%05d_%d_%d_%.2fms_%.2fm.bin", c->dump.iter, r->shot + 1, ns,
+                 ntr, s.dt * 1e3, s.dtr);
+        TRY(write_floats(c, name, p.data(), p.size()));
+        snprintf(name, sizeof name, "adjsource_iter%03d_shot%05d_%d_%d_%.2fms_%.2fm.bin", c->dump.iter, r->shot + 1, ns,
+                 ntr, s.dt * 1e3, s.dtr);
+        TRY(dump_device(c, name, c->d_pre[r->shot], (size_t)ns * ntr));
+    }
+    return FWI_OK;
+}
+
+// the raw shot gradient (mode 2's output, before the per-shot preconditioning) -- propagation.c:939-944
+static int dump_shot_gradients(fwi_ctx *c, const std::vector<ShotRun *> &rs)
+{
+    if (c->dump.verbose < 1) return FWI_OK;
+    char name[256];
+    for (ShotRun *r : rs) {
+        if (r->shot % c->dump.shot_interval != 0) continue;
+        snprintf(name, sizeof name, "gradient_raw_iter%03d_shot%05d_%d_%d_%.2fm_%.2fm.bin", c->dump.iter, r->shot + 1,
+                 c->nz, r->d.nxx, c->dz, c->dx);
+        TRY(dump_device(c, name, r->d_gshot, (size_t)c->nz * r->d.nxx));
+    }
+    return FWI_OK;
+}
+
+// snapshots after launch L of a program (verbose > 1): the forward field u(t) a forward step has
+// just written (t % snap_interval == 0; u(0) is the zero field), and at adjoint step it the adjoint
+// field with this step's injection and the reconstructed forward field the imaging reads
+// (propagation.c:597-601, 717-723).  Shots whose (shotID - 1) % shot_interval == 0, as the
+// reference's engine selects them.  The reference's reconstructed field at a step that is not an
+// imaging step (it % 5 != 0) is whatever its replay buffers last held; this engine keeps the
+// reconstructed field of imaging steps only, so that file is not written (with a warning) when
+// snap_interval is not a multiple of 5.
+static int snapshots_after(fwi_ctx *c, const Program *prog, int L, int shot_base, int nshot)
+{
+    const int snap = c->dump.snap_interval;
+    const int4 pw = prog->items[L];
+    char name[256];
+    for (int part = 0; part < 2; part++) {
+        const int kind = part ? pw.z : pw.x, it = part ? pw.w : pw.y;
+        if (kind == K_NONE || kind == K_REP) continue;
+        const bool fwd = kind == K_FWD0 || kind == K_FWD1;
+        const int t = fwd ? it + 1 : it;
+        const bool at0 = fwd && it == 0;  // u(0), the initial zero field, is a snapshot too
+        if (!at0 && (t >= c->nt || t % snap != 0)) continue;
+        for (int i = 0; i < nshot; i++) {
+            const ShotRun *r = c->runs.size() == 1 ? c->runs[0].get() : c->runs[shot_base + i].get();
+            const int ishot = c->shots[r->shot].s.shotID - 1;
+            if (ishot % c->dump.shot_interval != 0) continue;
+            const ShotDesc &d = r->d;
+            if (fwd) {
+                if (at0) {
+                    std::vector<float> z((size_t)d.Nx * d.Nz, 0.0f);
+                    snprintf(name, sizeof name, "wavefield_forward_iter%03d_ishot%04d_it%05d_%d_%d_%.2fm_%.2fm.bin",
+                             c->dump.iter, ishot, 0, d.Nz, d.Nx, c->dz, c->dx);
+                    TRY(write_floats(c, name, z.data(), z.size()));
+                }
+                if (t < c->nt && t % snap == 0) {
+                    snprintf(name, sizeof name, "wavefield_forward_iter%03d_ishot%04d_it%05d_%d_%d_%.2fm_%.2fm.bin",
+                             c->dump.iter, ishot, t, d.Nz, d.Nx, c->dz, c->dx);
+                    TRY(dump_frame(c, name, d, fwd_idx(d, t, kind == K_FWD1)));
+                }
+            } else {
+                if (it % MST == 0) {
+                    snprintf(name, sizeof name,
+                             "wavefield_forward_reconstruction_iter%03d_ishot%04d_it%05d_%d_%d_%.2fm_%.2fm.bin",
+                             c->dump.iter, ishot, it, d.Nz, d.Nx, c->dz, c->dx);
+                    TRY(dump_frame(c, name, d, img_idx(d, it)));
+                } else if (!c->dump.warned) {
+                    c->dump.warned = true;
+                    fprintf(stderr, "<warning>: snapInterval %d is not a multiple of %d: the reconstructed forward "
+                                    "wavefields of steps that are not imaging steps are not written\n", snap, MST);
+                }
+                snprintf(name, sizeof name, "wavefield_backward_iter%03d_ishot%04d_it%05d_%d_%d_%.2fm_%.2fm.bin",
+                         c->dump.iter, ishot, it, d.Nz, d.Nx, c->dz, c->dx);
+                TRY(dump_frame(c, name, d, adj_idx(d, it)));
+            }
+        }
+    }
+    return FWI_OK;
+}
+
+extern "C" int fwi_ctx_set_verbose(fwi_ctx *c, int verbose, int iter, int shot_interval, int snap_interval,
+                                   const char *dir)
+{
+    if (!c) return fail(FWI_ERR_ARG, "NULL context");
+    if (shot_interval <= 0) {  // the reference's environment variable, default 20 (propagation.c:846-852)
+        const char *e = getenv("shotInterval");
+        shot_interval = e ? atoi(e) : 20;
+    }
+    if (snap_interval <= 0) {  // propagation.c:432-440
+        const char *e = getenv("snapInterval");
+        snap_interval = e ? atoi(e) : 1000;
+    }
+    if (verbose > 0 && (shot_interval <= 0 || (verbose > 1 && snap_interval <= 0)))
+        return fail(FWI_ERR_ARG, "shotInterval %d / snapInterval %d must be positive", shot_interval, snap_interval);
+    if ((verbose > 1) != (c->dump.verbose > 1) || (verbose > 1 && snap_interval != c->dump.snap_interval))
+        drop_graphs(c);  // the step kernels' snapshot steps change
+    c->dump.verbose = verbose;
+    c->dump.iter = iter;
+    c->dump.shot_interval = shot_interval;
+    c->dump.snap_interval = snap_interval;
+    c->dump.dir = dir ? dir : "";
+    c->dump.warned = false;
+    return FWI_OK;
+}
+
 static int upload_descs(fwi_ctx *c, const std::vector<ShotDesc> &v)
 {
     if ((int)v.size() > c->desc_cap) {
@@ -1130,24 +1300,6 @@ static int gather(fwi_ctx *c, const std::vector<ShotRun *> &rs, int mode, bool w
 static __global__ void k_to_time_major(const float *__restrict__ a, float *__restrict__ out, int ntr, int ns, int nt);
 
 // ---------------------------------------------------------------- residual filters
-static int blas_ok(cublasStatus_t st, const char *what)
-{
-    if (st != CUBLAS_STATUS_SUCCESS) return fail(FWI_ERR_CUDA, "%s failed (cuBLAS status %d)", what, (int)st);
-    return FWI_OK;
-}
-
-static int get_blas(fwi_ctx *c, cublasHandle_t *out)
-{
-    if (!c->blas) {
-        TRY(blas_ok(cublasCreate(&c->blas), "cublasCreate"));
-        // plain FP32 products and sums: no TF32 or other reduced-precision modes
-        TRY(blas_ok(cublasSetMathMode(c->blas, CUBLAS_PEDANTIC_MATH), "cublasSetMathMode"));
-    }
-    TRY(blas_ok(cublasSetStream(c->blas, c->stream), "cublasSetStream"));
-    *out = c->blas;
-    return FWI_OK;
-}
-
 static std::string bits(float v)
 {
     uint32_t u;
@@ -1172,18 +1324,43 @@ static int device_operator(fwi_ctx *c, const std::string &key, size_t count, Bui
     return FWI_OK;
 }
 
-static int filter_operator(fwi_ctx *c, int filter, int n, float fpass, float fcut, float dt, const float **out)
+// The residual filters and the trace interpolation as FFT convolutions (fwi_fft.cuh): the
+// spectrum of the filter's circular kernel and the FFT twiddles, built once on the host in FP64
+// and kept on the device (2M floats each, M = fwi_conv_size(n)).
+static int conv_tables(fwi_ctx *c, const std::string &key, int n, const std::function<void(double *)> &kernel,
+                       ConvDesc *d)
+{
+    const int M = fwi_conv_size(n);
+    if (M > FFT_CONV_MAX)
+        return fail(FWI_ERR_UNSUPPORTED, "FFT convolution of length %d needs %d points (at most %d)", n, M,
+                    FFT_CONV_MAX);
+    const float *G, *tw;
+    TRY(device_operator(c, "spec/" + key, (size_t)2 * M, [&](float *out) {
+        std::vector<double> h(n);
+        kernel(h.data());
+        fwi_conv_spectrum(h.data(), n, M, out);
+    }, &G));
+    TRY(device_operator(c, "tw/" + std::to_string(M), (size_t)M, [&](float *out) { fwi_fft_twiddles(M, out); }, &tw));
+    d->G = (const float2 *)G;
+    d->tw = (const float2 *)tw;
+    d->N = n;
+    return FWI_OK;
+}
+
+// apply_traces_lowpass (filter 0) / apply_traces_bandpass (1) along `n`-sample sequences
+static int filter_tables(fwi_ctx *c, int filter, int n, float fpass, float fcut, float dt, ConvDesc *d)
 {
     const std::string key = "filter" + std::to_string(filter) + "/" + std::to_string(n) + "/" + bits(fpass) + "/" +
                             bits(fcut) + "/" + bits(dt);
-    return device_operator(c, key, (size_t)n * n,
-                           [&](float *h) { fwi_filter_operator(filter, n, fpass, fcut, dt, h); }, out);
+    return conv_tables(c, key, n, [&](double *h) { fwi_filter_kernel(filter, n, fpass, fcut, dt, h); }, d);
 }
 
-static int interp_operator(fwi_ctx *c, int ns, int r, int nt, const float **out)
+static int run_conv(fwi_ctx *c, const ConvDesc &d)
 {
-    const std::string key = "interp/" + std::to_string(ns) + "/" + std::to_string(r) + "/" + std::to_string(nt);
-    return device_operator(c, key, (size_t)nt * ns, [&](float *h) { fwi_interp_operator(ns, r, nt, h); }, out);
+    const cudaError_t e = launch_fft_conv(d, c->stream);
+    if (e != cudaSuccess) return fail(FWI_ERR_CUDA, "FFT convolution: %s", cudaGetErrorString(e));
+    c->launches++;
+    return FWI_OK;
 }
 
 static int taper(fwi_ctx *c, float *a, const ShotRun *r, int Lt, int Lr)
@@ -1199,16 +1376,14 @@ static int taper(fwi_ctx *c, float *a, const ShotRun *r, int Lt, int Lr)
 
 // compute_adjoint_source2d for filters 0/1 (optimization.c:368-415) and the injection layout for
 // sampleRate > 1 (interpolate_traces, common.c:482-582): residual and time taper in k_gather, then
-// per shot the time filter (GEMM with the ns x ns circulant), the trace taper, the trace filter
-// (GEMM with the shot's ntr x ntr circulant), both tapers; the adjoint source for the injection is
-// the interpolation GEMM into adj_t [nt][ntr] (or a transpose for sampleRate 1).
+// per shot the time filter (FFT convolution along each trace), the trace taper, the trace filter
+// (FFT convolution across the traces of each time sample), both tapers; the adjoint source for the
+// injection is the interpolation (FFT convolution of the zero-stuffed traces) written straight
+// into adj_t [nt][ntr], or a transpose for sampleRate 1.
 static int adjoint_source_filtered(fwi_ctx *c, const std::vector<ShotRun *> &rs, int filter, bool with_adj)
 {
     const bool fft = filter == 0 || filter == 1;
     TRY(gather(c, rs, 1, false, /*trace_taper=*/!fft));
-    cublasHandle_t h;
-    TRY(get_blas(c, &h));
-    const float one = 1.0f, zero = 0.0f;
     for (ShotRun *r : rs) {
         const int ns = r->d.ns, ntr = r->d.ntr;
         const fwi_shot &s = c->shots[r->shot].s;
@@ -1222,26 +1397,32 @@ static int adjoint_source_filtered(fwi_ctx *c, const std::vector<ShotRun *> &rs,
                 TRY(dmalloc(c, (void **)&c->d_fft_tmp, need));
                 c->fft_tmp_bytes = need;
             }
-            const float *Ct, *Cx;
-            TRY(filter_operator(c, filter, ns, r->fpass, 2.0f * r->fpass, s.dt, &Ct));
-            TRY(filter_operator(c, filter, ntr, r->kpass, 2.0f * r->kpass, s.dtr, &Cx));
-            // time filter: every trace (a column of the [ntr][ns] gather seen column-major) times Ct
-            TRY(blas_ok(cublasSgemm(h, CUBLAS_OP_N, CUBLAS_OP_N, ns, ntr, ns, &one, Ct, ns, pre, ns, &zero,
-                                    c->d_fft_tmp, ns), "time filter GEMM"));
+            // time filter: each trace, a row of the [ntr][ns] gather
+            ConvDesc t{};
+            TRY(filter_tables(c, filter, ns, r->fpass, 2.0f * r->fpass, s.dt, &t));
+            t.in = pre; t.in_es = 1; t.in_ss = ns; t.n_in = ns; t.stuff = 1;
+            t.out = c->d_fft_tmp; t.out_es = 1; t.out_ss = ns; t.n_out = ns; t.nseq = ntr;
+            TRY(run_conv(c, t));
             TRY(taper(c, c->d_fft_tmp, r, 0, r->Lr));
-            // trace filter: each time sample's vector over the traces times Cx (Cx is symmetric)
-            TRY(blas_ok(cublasSgemm(h, CUBLAS_OP_N, CUBLAS_OP_T, ns, ntr, ntr, &one, c->d_fft_tmp, ns, Cx, ntr, &zero,
-                                    pre, ns), "trace filter GEMM"));
+            // trace filter: each time sample's vector over the traces
+            ConvDesc x{};
+            TRY(filter_tables(c, filter, ntr, r->kpass, 2.0f * r->kpass, s.dtr, &x));
+            x.in = c->d_fft_tmp; x.in_es = ns; x.in_ss = 1; x.n_in = ntr; x.stuff = 1;
+            x.out = pre; x.out_es = ns; x.out_ss = 1; x.n_out = ntr; x.nseq = ns;
+            TRY(run_conv(c, x));
             TRY(taper(c, pre, r, r->Lt, r->Lr));
         }
         if (!with_adj) continue;
         float *adj = (float *)r->d.adj_t;
         if (r->d.sr > 1) {
-            const float *M;
-            TRY(interp_operator(c, ns, r->d.sr, c->nt, &M));
-            // adj_t[k][r] = sum_j M[k][j] pre[r][j]: the [nt][ntr] injection layout directly
-            TRY(blas_ok(cublasSgemm(h, CUBLAS_OP_T, CUBLAS_OP_T, ntr, c->nt, ns, &one, pre, ns, M, c->nt, &zero, adj,
-                                    ntr), "interpolation GEMM"));
+            // adj_t[k][r] = sum_j g[(k - j sr) mod N] pre[r][j] for k < N, 0 for N <= k < nt
+            const int sr = r->d.sr, N = (ns - 1) * sr + 1;
+            ConvDesc q{};
+            TRY(conv_tables(c, "interp/" + std::to_string(ns) + "/" + std::to_string(sr), N,
+                            [&](double *g) { fwi_interp_kernel(ns, sr, g); }, &q));
+            q.in = pre; q.in_es = 1; q.in_ss = ns; q.n_in = ns; q.stuff = sr;
+            q.out = adj; q.out_es = ntr; q.out_ss = 1; q.n_out = c->nt; q.nseq = ntr;
+            TRY(run_conv(c, q));
         } else {
             k_to_time_major<<<296, 256, 0, c->stream>>>(pre, adj, ntr, ns, c->nt);
             c->launches++;
@@ -1367,6 +1548,20 @@ static int stack_and_precondition(fwi_ctx *c, const std::vector<ShotRun *> &rs, 
     c->launches++;
     if (precondition == 1) {
         k_to_float<<<592, 256, 0, c->stream>>>(c->d_hc, c->d_prec, m);
+        c->launches++;
+    }
+    if (c->dump.verbose > 0) {  // the stacks before the global preconditioning (propagation.c:996-1005)
+        char name[256];
+        snprintf(name, sizeof name, "gradient_raw_iter%03d_%d_%d_%.2fm_%.2fm.bin", c->dump.iter, c->nz, c->nx, c->dz,
+                 c->dx);
+        TRY(dump_device(c, name, c->d_grad, (size_t)m));
+        if (precondition == 1) {
+            snprintf(name, sizeof name, "precond_iter%03d_%d_%d_%.2fm_%.2fm.bin", c->dump.iter, c->nz, c->nx, c->dz,
+                     c->dx);
+            TRY(dump_device(c, name, c->d_prec, (size_t)m));
+        }
+    }
+    if (precondition == 1) {
         SumDesc s{};
         s.a = c->d_prec;
         s.n = m;
@@ -1375,7 +1570,7 @@ static int stack_and_precondition(fwi_ctx *c, const std::vector<ShotRun *> &rs, 
         double *res;
         TRY(reduce(c, {s}, h, &res));
         k_global_precondition<<<592, 256, 0, c->stream>>>(c->d_grad, c->d_prec, m, res, 0.005f);
-        c->launches += 2;
+        c->launches++;
     }
     CK(cudaGetLastError());
     return FWI_OK;
@@ -1432,6 +1627,13 @@ static int run_program(fwi_ctx *c, const std::string &key, const Program *prog, 
     if (c->tune && tile_kernel && !getenv("FWI_TX") && !getenv("FWI_NST") && !getenv("FWI_CHUNK") && !getenv("FWI_GPT") &&
         !getenv("FWI_OCC"))
         TRY(autotune(c, shot_base, nshot, r0, batched));
+    if (c->dump.verbose > 1) {
+        // snapshots: direct launches with a copy-out after every snapshot step
+        c->snapping = true;
+        const int rc = launch_steps(c, prog, shot_base, nshot, r0, batched);
+        c->snapping = false;
+        return rc;
+    }
     if (!batched) return launch_steps(c, prog, shot_base, nshot, r0, false);
     if (!c->use_graphs) return launch_steps(c, prog, shot_base, nshot, r0, true);
     auto it = c->graphs.find(key);
@@ -1508,7 +1710,9 @@ static int run_gradient_group(fwi_ctx *c, std::vector<ShotRun *> &rs, float freq
     for (ShotRun *r : rs) interp = interp || r->d.sr > 1;
     if (filter == 2 && !interp) TRY(gather(c, rs, 1, true));  // residual + tapers straight into adj_t
     else TRY(adjoint_source_filtered(c, rs, filter, true));
+    TRY(dump_shot_traces(c, rs));
     TRY(grad_adjoint(c, rs, batched, gkey, shot_base));
+    TRY(dump_shot_gradients(c, rs));
     if (precondition == 1) TRY(shot_precondition(c, rs));
     return FWI_OK;
 }
@@ -1801,9 +2005,11 @@ extern "C" size_t fwi_estimate_bytes(const fwi_shot *shots, int nshot, int nz, i
         const size_t Nx = (size_t)(w.second - w.first + 1) + 2 * pml, Nz = (size_t)nz + 2 * pml;
         b += 6 * Nx * ((Nz + 3) / 4 * 4) * 4;  // coefficient planes of the window
     }
-    if ((grad || problem == 2) && (filter == 0 || filter == 1))
-        b += max_ns * max_ntr * 4 + max_ns * max_ns * 4 + (size_t)nshot * max_ntr * max_ntr * 4;
-    if (grad) b += (size_t)nt * max_ns * 4;  // interpolation operator (sampleRate > 1)
+    // FFT convolution tables: spectra and twiddles of the time and trace filters and of the
+    // interpolation (2 M floats each), and the filters' intermediate gather
+    const size_t Mt = (size_t)fwi_conv_size((int)std::max(max_ns, (size_t)nt)), Mx = (size_t)fwi_conv_size((int)max_ntr);
+    if ((grad || problem == 2) && (filter == 0 || filter == 1)) b += max_ns * max_ntr * 4 + 8 * (Mt + Mx) * 4;
+    if (grad) b += 4 * Mt * 4;
     b += (size_t)nshot * sizeof(ShotDesc) + ((size_t)3 * nt + 64) * sizeof(int4) + (8u << 20);
     return b + b / 20 + (96u << 20);  // 5 % and 96 MiB for the library workspaces and graphs
 }
@@ -1891,8 +2097,6 @@ extern "C" int fwi_iso_acoustic2d_propagation_engine(Record2D *r, Acoustic2dChec
                                                      int fs, int precondition, int mode, int iter, int verbose,
                                                      float **grad)
 {
-    (void)iter;
-    (void)verbose;
     if (!r || !vpm || !rhom || mode < 0 || mode > 2) return fail(FWI_ERR_ARG, "invalid engine arguments");
     if (!rows_contiguous(vpm, nz, nx) || !rows_contiguous(rhom, nz, nx))
         return fail(FWI_ERR_ARG, "vpm/rhom must be one contiguous block (alloc2float layout)");
@@ -1907,6 +2111,8 @@ extern "C" int fwi_iso_acoustic2d_propagation_engine(Record2D *r, Acoustic2dChec
         if (!k->ctx) TRY(fwi_ctx_create(&k->ctx, 0, 0));
         c = k->ctx;
     }
+    // the engine writes only snapshots (verbose > 1); the per-shot files are the driver's
+    TRY(fwi_ctx_set_verbose(c, verbose > 1 ? verbose : 0, iter, 0, 0, nullptr));
     fwi_shot s{};
     s.shotID = r->shotID; s.isx = r->isx; s.isz = r->isz; s.ntr = r->ntr; s.ns = r->ns;
     s.sampleRate = r->sampleRate; s.ix_min = 0; s.ix_max = nx - 1;  // vpm is the shot's window already

@@ -49,6 +49,9 @@ struct ShotDesc {
     double *H, *Gacc;      // [Nx][ld] FP64 accumulators (pseudo-Hessian, gradient)
     long long frame;       // Nx*ld
     int rz0, rz1;          // padded depth range of this shot's receivers
+    int snap;              // > 0: steps whose output time is a multiple of snap mirror every free-surface
+                           // row (pml-1 .. 0), as the reference's snapshots hold them; 0: only the
+                           // three rows the stencil reads again
 };
 
 // ------------------------------------------------------------ buffer selection

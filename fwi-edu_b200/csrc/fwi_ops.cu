@@ -18,6 +18,7 @@
 #include "../../include/fwi_b200.h"
 #include "fwi_aux.cuh"
 #include "fwi_optim.cuh"
+#include "fwi_fft.cuh"
 #include "fwi_setup.h"
 
 using namespace fwi;
@@ -68,7 +69,7 @@ bool ops_ready(size_t bytes)
 
 size_t al(size_t b) { return (b + 255) & ~size_t(255); }
 
-// ---- residual filters and interpolation: operator matrices on the device, applied by FP32 GEMM
+// ---- operator matrices of the 2-D wavenumber filters, applied by FP32 GEMM
 cublasHandle_t g_blas = nullptr;
 std::map<std::string, float *> g_opmats;  // built once per (kind, size, parameters) and kept
 
@@ -105,28 +106,60 @@ const float *op_matrix(const std::string &key, size_t count, void (*build)(float
     return d;
 }
 
-void build_filter(float *h, const int *ip, const float *fp) { fwi_filter_operator(ip[0], ip[1], fp[0], fp[1], fp[2], h); }
-void build_interp(float *h, const int *ip, const float *) { fwi_interp_operator(ip[0], ip[1], ip[2], h); }
+// ---- residual filters and interpolation: FFT convolutions (fwi_fft.cuh) with the kernel's
+// spectrum and the twiddles built once on the host (FP64) and kept on the device
+struct Kernel1d {
+    int kind;  // 0 / 1: apply_traces_lowpass / _bandpass of length n; 2: interpolate_traces from ns by r
+    int n, r;
+    float fpass, fcut, dt;
+};
 
-// the n x n filter operator of apply_traces_lowpass (0) / apply_traces_bandpass (1)
-const float *filter_matrix(int filter, int n, float fpass, float fcut, float dt)
+void build_spectrum(float *out, const int *ip, const float *fp)
 {
-    const int ip[2] = {filter, n};
-    const float fp[3] = {fpass, fcut, dt};
-    return op_matrix("f" + std::to_string(filter) + "/" + std::to_string(n) + "/" + fbits(fpass) + "/" + fbits(fcut) +
-                         "/" + fbits(dt),
-                     (size_t)n * n, build_filter, ip, fp);
+    const int kind = ip[0], n = ip[1], r = ip[2], N = ip[3], M = fwi_conv_size(N);
+    std::vector<double> h(N);
+    if (kind == 2) fwi_interp_kernel(n, r, h.data());
+    else fwi_filter_kernel(kind, n, fp[0], fp[1], fp[2], h.data());
+    fwi_conv_spectrum(h.data(), N, M, out);
+}
+void build_twiddles(float *out, const int *ip, const float *) { fwi_fft_twiddles(ip[0], out); }
+
+// the tables of a convolution of length N into d; false (with a message) when N is too long
+bool conv_tables(const Kernel1d &k, int N, ConvDesc *d)
+{
+    const int M = fwi_conv_size(N);
+    if (M > FFT_CONV_MAX) {
+        fprintf(stderr, "<error>: FFT convolution of length %d needs %d points (at most %d)\n", N, M, FFT_CONV_MAX);
+        return false;
+    }
+    const int ip[4] = {k.kind, k.n, k.r, N};
+    const float fp[3] = {k.fpass, k.fcut, k.dt};
+    const float *G = op_matrix("s" + std::to_string(k.kind) + "/" + std::to_string(k.n) + "/" + std::to_string(k.r) +
+                                   "/" + fbits(k.fpass) + "/" + fbits(k.fcut) + "/" + fbits(k.dt),
+                               (size_t)2 * M, build_spectrum, ip, fp);
+    const int ipt[1] = {M};
+    const float *tw = op_matrix("tw/" + std::to_string(M), (size_t)M, build_twiddles, ipt, nullptr);
+    if (!G || !tw) return false;
+    d->G = (const float2 *)G;
+    d->tw = (const float2 *)tw;
+    d->N = N;
+    return true;
 }
 
-// y (ntr vectors of n samples, contiguous) = filter applied to x, both on the device
-bool filter_vectors(const float *x, float *y, int n, int nvec, int filter, float fpass, float fcut, float dt)
+bool run_conv(const ConvDesc &d, const char *what)
 {
-    if (!blas_ready()) return false;
-    const float *C = filter_matrix(filter, n, fpass, fcut, dt);
-    if (!C) return false;
-    const float one = 1.0f, zero = 0.0f;
-    return cublasSgemm(g_blas, CUBLAS_OP_N, CUBLAS_OP_N, n, nvec, n, &one, C, n, x, n, &zero, y, n) ==
-           CUBLAS_STATUS_SUCCESS;
+    return report(launch_fft_conv(d, g_ops.st), what);
+}
+
+// y (nvec sequences of n samples at element stride es, sequence stride ss) = filter applied to x
+bool filter_vectors(const float *x, float *y, int n, int nvec, long long es, long long ss, int filter, float fpass,
+                    float fcut, float dt)
+{
+    ConvDesc d{};
+    if (!conv_tables({filter, n, 1, fpass, fcut, dt}, n, &d)) return false;
+    d.in = x; d.in_es = es; d.in_ss = ss; d.n_in = n; d.stuff = 1;
+    d.out = y; d.out_es = es; d.out_ss = ss; d.n_out = n; d.nseq = nvec;
+    return run_conv(d, "FFT convolution");
 }
 
 // the taper of taper_traces (common.c:796-895) on a [ntr][ns] device gather
@@ -136,16 +169,6 @@ bool taper_device(float *a, int ns, int ntr, int Lt, int Lr, const float *tct, c
     if (!report(cudaMemcpyAsync(d, &t, sizeof(t), cudaMemcpyHostToDevice, g_ops.st), "copy")) return false;
     k_taper<<<dim3(148, 1), 256, 0, g_ops.st>>>(d);
     return report(cudaGetLastError(), "k_taper");
-}
-
-// [a][b] -> [b][a] on the device
-__global__ void k_transpose(const float *__restrict__ in, float *__restrict__ out, int a, int b)
-{
-    const long long n = (long long)a * b;
-    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
-        const int ib = (int)(i / a), ia = (int)(i % a);
-        out[i] = in[(long long)ia * b + ib];
-    }
 }
 
 // FP64 sums of one or two operand arrays already on the device
@@ -261,7 +284,7 @@ extern "C" void smooth2D(float **in, float **out, int nx, int nz, int N, int isz
 }
 
 // compute_adjoint_source2d, optimization.c:300-419: residual; for filters 0/1 the time taper, time
-// filter, trace taper and trace filter (GEMMs with the circulant operators); both tapers
+// filter, trace taper and trace filter (FFT convolutions); both tapers
 extern "C" void compute_adjoint_source2d(Record2D *pre, Record2D *obs, float **vp, float freq, int filter,
                                          Record2D *adj)
 {
@@ -301,17 +324,15 @@ extern "C" void compute_adjoint_source2d(Record2D *pre, Record2D *obs, float **v
     } else {
         k_residual_taper<<<296, 256, 0, g_ops.st>>>(dp, dob, da, ns, ntr, Lt, 0, dt_, dr);
         // time filter of every trace, trace taper, filter along the traces of every sample, tapers
-        if (!filter_vectors(da, dp, ns, ntr, filter, freq, 2.0f * freq, adj->dt)) {
+        if (!filter_vectors(da, dp, ns, ntr, 1, ns, filter, freq, 2.0f * freq, adj->dt)) {
             fprintf(stderr, "<error>: compute_adjoint_source2d: time filter failed\n");
             return;
         }
         if (!taper_device(dp, ns, ntr, 0, Lr, dt_, dr, td)) return;
-        k_transpose<<<296, 256, 0, g_ops.st>>>(dp, dob, ntr, ns);  // [ntr][ns] -> [ns][ntr]
-        if (!filter_vectors(dob, da, ntr, ns, filter, kpass, 2.0f * kpass, adj->dtr)) {
+        if (!filter_vectors(dp, dp, ntr, ns, ns, 1, filter, kpass, 2.0f * kpass, adj->dtr)) {
             fprintf(stderr, "<error>: compute_adjoint_source2d: trace filter failed\n");
             return;
         }
-        k_transpose<<<296, 256, 0, g_ops.st>>>(da, dp, ns, ntr);  // back to [ntr][ns]
         cudaStreamSynchronize(g_ops.st);  // the taper descriptor is reused
         if (!taper_device(dp, ns, ntr, Lt, Lr, dt_, dr, td)) return;
         da = dp;
@@ -338,8 +359,8 @@ static void traces_filter(float **tr, float **trs, int nt, int ntr, float fpass,
     if (!ops_ready(2 * nb)) return;
     float *x = (float *)g_ops.buf, *y = (float *)(g_ops.buf + nb);
     cudaMemcpyAsync(x, tr[0], m * 4, cudaMemcpyHostToDevice, g_ops.st);
-    if (!filter_vectors(x, y, nt, ntr, filter, fpass, fcut, dt)) {
-        fprintf(stderr, "<error>: %s: filter GEMM failed\n", name);
+    if (!filter_vectors(x, y, nt, ntr, 1, nt, filter, fpass, fcut, dt)) {
+        fprintf(stderr, "<error>: %s: FFT convolution failed\n", name);
         return;
     }
     cudaMemcpyAsync(trs[0], y, m * 4, cudaMemcpyDeviceToHost, g_ops.st);
@@ -370,20 +391,15 @@ extern "C" void interpolate_traces(float **tr, int ntr, int nt, int r, float **t
     }
     const int ns = (nt - 1) * r + 1;
     const size_t nb = al((size_t)nt * ntr * 4);
-    if (!ops_ready(nb + al((size_t)ns * ntr * 4)) || !blas_ready()) return;
+    if (!ops_ready(nb + al((size_t)ns * ntr * 4))) return;
     float *x = (float *)g_ops.buf, *y = (float *)(g_ops.buf + nb);
-    const int ip[3] = {nt, r, ns};
-    const float *M = op_matrix("i/" + std::to_string(nt) + "/" + std::to_string(r), (size_t)ns * nt, build_interp, ip,
-                               nullptr);
-    if (!M) return;
+    ConvDesc d{};
+    if (!conv_tables({2, nt, r, 0.f, 0.f, 0.f}, ns, &d)) return;
     cudaMemcpyAsync(x, tr[0], sizeof(float) * (size_t)nt * ntr, cudaMemcpyHostToDevice, g_ops.st);
-    const float one = 1.0f, zero = 0.0f;
-    // y[itr] = M x[itr]: each trace a column of length nt, each output a column of length ns
-    if (cublasSgemm(g_blas, CUBLAS_OP_N, CUBLAS_OP_N, ns, ntr, nt, &one, M, ns, x, nt, &zero, y, ns) !=
-        CUBLAS_STATUS_SUCCESS) {
-        fprintf(stderr, "<error>: interpolate_traces: GEMM failed\n");
-        return;
-    }
+    // each trace zero-stuffed by r and convolved with the band window's kernel
+    d.in = x; d.in_es = 1; d.in_ss = nt; d.n_in = nt; d.stuff = r;
+    d.out = y; d.out_es = 1; d.out_ss = ns; d.n_out = ns; d.nseq = ntr;
+    if (!run_conv(d, "interpolate_traces")) return;
     cudaMemcpyAsync(trs[0], y, sizeof(float) * (size_t)ns * ntr, cudaMemcpyDeviceToHost, g_ops.st);
     report(cudaStreamSynchronize(g_ops.st), "interpolate_traces");
 }

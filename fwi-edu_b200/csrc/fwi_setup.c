@@ -343,6 +343,93 @@ void fwi_filter_operator(int filter, int n, float fpass, float fcut, float dt, f
     free(h);
 }
 
+/* ------------------------------------------------------------ FFT convolution spectra */
+/* in-place radix-2 FFT of n = 2^k complex doubles (sign -1: forward, +1: inverse, unscaled) */
+static void fft_pow2(double *re, double *im, int n, int sign)
+{
+    for (int i = 1, j = 0; i < n; i++) { /* bit reversal */
+        int bit = n >> 1;
+        for (; j & bit; bit >>= 1) j ^= bit;
+        j ^= bit;
+        if (i < j) {
+            double t = re[i]; re[i] = re[j]; re[j] = t;
+            t = im[i]; im[i] = im[j]; im[j] = t;
+        }
+    }
+    for (int len = 2; len <= n; len <<= 1) {
+        const double ang = sign * 2.0 * 3.141592653589793 / len;
+        for (int k = 0; k < len / 2; k++) {
+            const double wr = cos(ang * k), wi = sin(ang * k);
+            for (int i = k; i < n; i += len) {
+                const int j = i + len / 2;
+                const double xr = re[j] * wr - im[j] * wi, xi = re[j] * wi + im[j] * wr;
+                re[j] = re[i] - xr; im[j] = im[i] - xi;
+                re[i] += xr; im[i] += xi;
+            }
+        }
+    }
+}
+
+int fwi_conv_size(int n)
+{
+    int M = 2;
+    while (M < 2 * n - 1) M <<= 1;
+    return M;
+}
+
+void fwi_conv_spectrum(const double *h, int n, int M, float *G)
+{
+    double *re = (double *)calloc((size_t)M, sizeof(double)), *im = (double *)calloc((size_t)M, sizeof(double));
+    for (int m = 0; m < n; m++) re[m] = h[m];
+    for (int m = 1; m < n; m++) re[M - m] = h[n - m];
+    fft_pow2(re, im, M, -1);
+    for (int k = 0; k < M; k++) {
+        G[2 * k] = (float)(re[k] / M);
+        G[2 * k + 1] = (float)(im[k] / M);
+    }
+    free(re);
+    free(im);
+}
+
+void fwi_fft_twiddles(int M, float *tw)
+{
+    for (int k = 0; k < M / 2; k++) {
+        const double a = 2.0 * 3.141592653589793 * k / M;
+        tw[2 * k] = (float)cos(a);
+        tw[2 * k + 1] = (float)-sin(a);
+    }
+}
+
+void fwi_filter_kernel(int filter, int n, float fpass, float fcut, float dt, double *h)
+{
+    float *win = (float *)malloc(sizeof(float) * (size_t)n);
+    fwi_filter_window(filter, n, fpass, fcut, dt, win);
+    circular_kernel(win, n, h);
+    free(win);
+}
+
+void fwi_interp_kernel(int ns, int r, double *g)
+{
+    const int N = (ns - 1) * r + 1, nkeep = N / (2 * r);
+    float *win = (float *)calloc((size_t)N, sizeof(float));
+    for (int k = 0; k < nkeep; k++) win[k] = (float)r;
+    for (int k = N - nkeep + 1; k < N; k++) win[k] = (float)r;
+    double *cs = (double *)malloc(sizeof(double) * (size_t)N);
+    for (int m = 0; m < N; m++) cs[m] = cos(2.0 * 3.141592653589793 * m / N);
+    for (int m = 0; m < N; m++) {
+        double a = 0.0;
+        int idx = 0;
+        for (int k = 0; k < N; k++) {
+            a += (double)win[k] * cs[idx];
+            idx += m;
+            if (idx >= N) idx -= N;
+        }
+        g[m] = a / N;
+    }
+    free(win);
+    free(cs);
+}
+
 /* zero-stuffing by r, a rectangular window of height r on |k| < N / (2r) of the length-N
  * spectrum (N = (ns - 1) r + 1), inverse FFT, real part / N:  y[i] = sum_j x[j] g[(i - j r) mod N] */
 void fwi_interp_operator(int ns, int r, int nt, float *M)

@@ -53,6 +53,20 @@ void fwi_filter_window(int filter, int n, float fpass, float fcut, float dt, flo
 void fwi_filter_operator(int filter, int n, float fpass, float fcut, float dt, float *C);
 void fwi_interp_operator(int ns, int r, int nt, float *M);
 
+/* The same filters and the interpolation as circular convolutions applied by FFT on the device.
+ * fwi_filter_kernel: h[0..n) of apply_traces_lowpass/bandpass, the length-n circular kernel
+ *   y[i] = sum_j h[(i - j) mod n] x[j] (FP64);
+ * fwi_interp_kernel: g[0..N), N = (ns - 1) r + 1, of interpolate_traces: y[i] = sum_j g[(i - j r) mod N] x[j];
+ * fwi_conv_size: M = the power of two >= 2n - 1, so that an M-point circular convolution of the
+ *   zero-padded signal with the wrapped kernel equals the n-point one on [0, n);
+ * fwi_conv_spectrum: G = FFT_M(wrapped h) / M, M complex floats as (re, im) pairs (FP64 FFT);
+ * fwi_fft_twiddles: exp(-2 pi i k / M), k < M / 2, as (re, im) float pairs. */
+void fwi_filter_kernel(int filter, int n, float fpass, float fcut, float dt, double *h);
+void fwi_interp_kernel(int ns, int r, double *g);
+int fwi_conv_size(int n);
+void fwi_conv_spectrum(const double *h, int n, int M, float *G);
+void fwi_fft_twiddles(int M, float *tw);
+
 /* lowpass2d (filter 0, common.c:1042-1162) / bandpass2d (filter 1, :1164-1284) window over the
  * full Nx x Nz wavenumber plane of the padded field, W[ix * Nz + iz], from the reference's float
  * expressions (generate_frequency, common.c:333-361).

@@ -407,8 +407,11 @@ __device__ __forceinline__ void tile_body(const CUtensorMap &tm_p1, const CUtens
     // pml-1..0 (propagation.c:76-101).  Only the three mirrored rows next to the surface are ever
     // read again (the stencil updates rows >= pml and reaches three rows up; receivers, imaging
     // and the Hessian lie at rows >= pml), so only rows pml+1..pml+3 are mirrored here: every
-    // seismogram and gradient is the reference's, and the rows above pml-3 are never written.
-    const int fs_hi = min(2 * pml, pml + 3);  // last mirrored source row
+    // seismogram and gradient is the reference's, and the rows above pml-3 are never written --
+    // except on the steps whose output field is written out as a snapshot (A.snap), which
+    // mirror all pml rows so that the snapshot holds what the reference's field holds.
+    const int tout = kind == K_ADJ ? it - 1 : it + 1;  // time index of the field this step writes
+    const int fs_hi = (A.snap > 0 && tout % A.snap == 0) ? 2 * pml : min(2 * pml, pml + 3);  // last mirrored source row
     const bool inject = kind == K_ADJ && it >= 1;
     const bool hess = kind == K_FWD1 && A.hessian && (it % MST == 0);
     const bool image = kind == K_ADJ && (it % MST == 0);

@@ -264,6 +264,14 @@ class Context:
         _check(self.L.fwi_ctx_get_model(self.h, _ptr(vp), _ptr(rho)))
         return vp, rho
 
+    def set_verbose(self, verbose, iteration=1, shot_interval=0, snap_interval=0, directory=None):
+        """The reference's intermediate files (fwi_ctx_set_verbose): verbose 1 per-shot traces and
+        gradients and the stacked gradient of a gradient run, verbose 2 also wavefield snapshots.
+        Intervals <= 0 come from the shotInterval / snapInterval environment variables."""
+        d = None if directory is None else str(directory).encode()
+        _check(self.L.fwi_ctx_set_verbose(self.h, int(verbose), int(iteration), int(shot_interval),
+                                          int(snap_interval), d))
+
     def set_allreduce(self, fn):
         """Install the exchange hook of a shot-sharded run (fwi_ctx_set_allreduce).
 

@@ -216,6 +216,21 @@ FWI_API int fwi_ctx_launch_variant(fwi_ctx *ctx, int *groups_per_thread, int *bl
  * off, every step is launched directly -- cheaper for a launch sequence run only once. */
 FWI_API int fwi_ctx_set_graphs(fwi_ctx *ctx, int on);
 
+/* The reference's verbose output (replaces the `verbose`/`iter` arguments and the shotInterval /
+ * snapInterval environment variables of iso_acoustic2d_propagation, propagation.c:423-441,
+ * 846-852).  verbose >= 1: a gradient run (problem 1) writes, for every shot_interval-th shot,
+ * predicted_iter*_shot*.bin, adjsource_iter*_shot*.bin and gradient_raw_iter*_shot*.bin, and
+ * per gradient gradient_raw_iter*.bin and precond_iter*.bin (propagation.c:917-944, 996-1005);
+ * verbose > 1: also wavefield snapshots every snap_interval steps of the shots whose
+ * (shotID - 1) % shot_interval == 0 (wavefield_forward*, wavefield_forward_reconstruction*,
+ * wavefield_backward*, propagation.c:597-601, 717-723; the reconstructed field is written at
+ * imaging steps, multiples of 5).  Raw float32 files with the reference's names, in `dir` (NULL:
+ * the working directory, as the reference).  shot_interval / snap_interval <= 0: read from the
+ * environment variables shotInterval / snapInterval, defaults 20 / 1000.  Snapshot runs launch
+ * the step kernel directly (no CUDA graphs) and copy every snapshot out as it is produced. */
+FWI_API int fwi_ctx_set_verbose(fwi_ctx *ctx, int verbose, int iter, int shot_interval, int snap_interval,
+                                const char *dir);
+
 /* Device bytes a context needs for one run of `problem` (0 modeling, 1 gradient, 2 line-search
  * residual) over these shots of an nz x nx model: what a serving loop admits requests by.
  * No counterpart in the reference. */
@@ -317,14 +332,23 @@ FWI_API int fwi_ctx_get_model(fwi_ctx *ctx, float *vp, float *rho);
  * counterpart in the reference.  It is meant for callers that cannot call cudaMalloc: a serving
  * loop that has reserved its whole device budget up front, host code that runs between the
  * segments of a captured CUDA graph, or a latency-critical loop where an allocation would
- * synchronise the device.  d_in and d_out are the caller's device arrays (they may not overlap);
- * the intermediate field lives in a file-scope device array of 4194304 floats (16 MiB) that every
+ * synchronise the device.  d_in and d_out are the caller's device arrays (the same array smooths
+ * in place; partly overlapping arrays are not allowed); the intermediate field lives in a file-scope device array of 4194304 floats (16 MiB) that every
  * GPU loading this library holds until the process exits.  nx*nz above 4194304 or half-widths
  * outside [1, 32] are rejected with FWI_ERR_ARG and a message.  The first call on a device looks up
  * the array's address on that device (with that device current): make that first call before any
- * stream capture.  All calls share the array, so calls that overlap on the GPU race on it.
+ * stream capture.  The address found then belongs to that CUDA context: after a cudaDeviceReset
+ * the process must not call this entry point again.  All calls share the array, so calls that
+ * overlap on the GPU race on it.
  * stream is a cudaStream_t (NULL: the legacy default stream); the call only enqueues work. */
 FWI_API int fwi_smooth2d_noalloc(const float *d_in, float *d_out, int nx, int nz, int rz, int rx, void *stream);
+
+/* Measurement helper (no counterpart in the reference): the L2 bandwidth figure that bounds the
+ * plain one-shot-per-launch path, whose per-shot state stays in L2.  Copies `bytes` between the
+ * device buffers d_a and d_b (each `bytes` long, 16-byte aligned, small enough that both stay in
+ * L2) `passes` times inside one kernel launch, alternating direction; *ms_out = device time of
+ * that launch (CUDA events on `stream`).  Bytes moved = 2 * bytes * passes. */
+FWI_API int fwi_l2_copy_probe(void *d_a, void *d_b, long long bytes, int passes, void *stream, float *ms_out);
 
 /* the launch program of one shot's adjoint pass (host-only, no device needed): four ints per
  * launch {kindA, stepA, kindB, stepB} with kinds 0 none, 3 replay step, 4 adjoint step.

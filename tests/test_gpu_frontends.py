@@ -102,9 +102,14 @@ def test_fwi_front_end_matches_reference(tmp_path, sched):
     fft = "0" in sched["filter"]
     tol_model, tol_grad = (1e-5, 1e-4) if fft else (1e-6, 1e-6)
     niter = sum(int(x) for x in sched["iteration"].split(","))
+    # verbose = 1: the same set of files as the reference writes, the engine's intermediate
+    # files (propagation.c:917-944, 996-1005) included
+    assert sorted(os.listdir(res["strict"])) == sorted(os.listdir(res["b200"]))
     for pattern, tol in (("vp_inversion_*.bin", tol_model), ("rho_inversion_*.bin", tol_model),
                          (f"objective_function_{niter:03d}.bin", tol_model), ("grad_iter*.bin", tol_grad),
-                         ("vp_iter*.bin", tol_model)):
+                         ("vp_iter*.bin", tol_model), ("predicted_iter*_shot*.bin", tol_model),
+                         ("adjsource_iter*_shot*.bin", tol_grad), ("gradient_raw_iter*_shot*.bin", tol_grad),
+                         ("gradient_raw_iter???_*_*.bin", tol_grad), ("precond_iter*.bin", tol_grad)):
         fa = sorted(glob.glob(str(res["strict"] / pattern)))
         fb = sorted(glob.glob(str(res["b200"] / pattern)))
         assert fa and [os.path.basename(x) for x in fa] == [os.path.basename(x) for x in fb], pattern
@@ -112,3 +117,40 @@ def test_fwi_front_end_matches_reference(tmp_path, sched):
             x, y = np.fromfile(b, np.float32), np.fromfile(a, np.float32)
             assert x.shape == y.shape and np.isfinite(x).all()
             assert rel(x, y) <= tol, f"{os.path.basename(a)}: rel {rel(x, y):.2e}"
+            if not fft and "shot" in os.path.basename(a):
+                # the first iteration's per-shot files come from the same model: bit for bit
+                if "_iter001_" in os.path.basename(a):
+                    assert np.array_equal(x, y), os.path.basename(a)
+
+
+def test_snapshots_match_reference(tmp_path):
+    """verbose = 2: wavefield snapshots every snapInterval steps (propagation.c:597-601, 717-723) --
+    forward fields of the modeling and gradient passes, the reconstructed forward field and the
+    adjoint field of the adjoint pass, with every free-surface row mirrored (the rows the
+    stencil never reads again included) -- identical to the reference's files, bit for bit."""
+    need_exes()
+    paths = inputs(tmp_path)
+    geom = dict(fsx=4, ds=25, sdepth=2, offsmin=0, offsmax=NX - 1, dtr=1, gdepth=2, sampleRate=1)
+    record = model_both(tmp_path, paths, **geom)["strict"][0]
+    env = dict(os.environ, snapInterval="100", shotInterval="2")
+    res = {}
+    for v in ("strict", "b200"):
+        d = tmp_path / f"snap_{v}"
+        d.mkdir()
+        params = dict(COMMON, verbose=2, srcfile=paths["src"], vpfile=paths["vp0"], recordfile=record, vpmin=1500.0,
+                      vpmax=4700.0, rhomin=1000.0, rhomax=2700.0, precondition=1, freq="10", filter="2",
+                      iteration="1", rx="1", rz="1", **geom)
+        args = [EXE[("fwi", v)]] + [f"{k}={val}" for k, val in params.items()]
+        p = subprocess.run(args, cwd=d, env=dict(env, OMP_NUM_THREADS="1"), capture_output=True, text=True,
+                           timeout=600)
+        assert p.returncode == 0, p.stdout[-2000:] + p.stderr[-2000:]
+        res[v] = d
+    names = sorted(os.listdir(res["strict"]))
+    assert names == sorted(os.listdir(res["b200"]))
+    snaps = [n for n in names if n.startswith("wavefield_")]
+    kinds = {n.split("_iter")[0] for n in snaps}
+    assert kinds == {"wavefield_forward", "wavefield_forward_reconstruction", "wavefield_backward"}, kinds
+    for n in snaps:
+        a = np.fromfile(res["strict"] / n, np.float32)
+        b = np.fromfile(res["b200"] / n, np.float32)
+        assert a.shape == b.shape and np.array_equal(a, b), f"{n}: rel {rel(b, a):.2e}"
