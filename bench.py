@@ -555,6 +555,67 @@ def step_roofline(ctx, E, peaks):
             "launch_shape": shape}
 
 
+def adjoint_roofline(ctx, E, peaks):
+    """The step kernel in the adjoint pass of a batched gradient (60 shots): each launch advances
+    every shot one replay step (forward reconstruction from the checkpoints) and one adjoint step
+    (with the imaging condition on every 5th step), device time from the engine's per-pass CUDA
+    events.  Algorithmic bytes over the pass: per shot-cell and step 12 B of fields + 24 B of
+    coefficients / S for every replay and adjoint step, plus 20 B on imaging steps (u read 4 B,
+    FP64 gradient accumulator read + write 16 B)."""
+    ctx.run(1, ITER["freq"], ITER["filter"], 1, E.PATH_BATCHED)
+    ctx.run(1, ITER["freq"], ITER["filter"], 1, E.PATH_BATCHED)
+    ps, st = ctx.pass_stats(), ctx.stats()
+    S = NSHOT
+    # cell_updates of a gradient run = shot-cells x (forward nt + replay n_rep + adjoint nt)
+    shot_cells = S * (NZ + 2 * PML) * (NX + 2 * PML)  # every shot's window spans the model
+    n_rep = st["cell_updates"] / shot_cells - 2 * NT
+    n_img = (NT - 1) // 5 + 1  # imaging steps, over the nz x nx interior of every shot
+    total = shot_cells * (n_rep + NT) * (12.0 + 24.0 / S) + S * NZ * NX * n_img * 20.0
+    achieved = total / (ps["adj_ms"] * 1e-3) / 1e9
+    peak = peaks.get("hbm_gbs")
+    return {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+            "frac": achieved / peak if peak else None,
+            "kernel": "k_tile (batched adjoint pass: replay step + adjoint step per launch, 60 shots)",
+            "launch_us": ps["adj_ms"] * 1e3 / max(ps["adj_launches"], 1), "launches": ps["adj_launches"],
+            "replay_steps_per_shot": n_rep, "algorithmic_bytes_per_pass": total,
+            "gcells_per_s": shot_cells * (n_rep + NT) / (ps["adj_ms"] * 1e-3) / 1e9,
+            "forward_pass_ms": ps["fwd_ms"], "adjoint_pass_ms": ps["adj_ms"],
+            "peak_source": "fallback" if peaks.get("fallback") else "measured"}
+
+
+def fp64_error(E, vp, rho, vp0, rho0, shots, local=0):
+    """The engine's FP32 results against an FP64 build of the same algorithm (the oracle's
+    restatement compiled with double, oracle/libfwi_oracle_f64.so) on one shot of the survey:
+    seismogram of the true model and the gradient of the starting model (problem 1)."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import pyoracle as po
+    os.environ["OMP_NUM_THREADS"] = str(os.cpu_count())
+    sh = [shots[len(shots) // 2]]
+    p64 = po.Port(64)
+    ctx = E.Context(local)
+    try:
+        ctx.set_model(vp, rho, DX, DX, DT, NT, PML, FS)
+        ctx.set_shots(sh)
+        ctx.run(0, path=E.PATH_BATCHED)
+        obs = [ctx.traces(0)]
+        ctx.set_model(vp0, rho0, DX, DX, DT, NT, PML, FS)
+        ctx.set_observed(obs)
+        ctx.run(1, ITER["freq"], ITER["filter"], 1, E.PATH_BATCHED)
+        g32 = ctx.gradient()
+    finally:
+        ctx.close()
+    o64, _ = p64.propagation(vp, rho, sh, DX, DX, DT, NT, PML, FS, 0.0, 2.0, 1, 0)
+    _, g64 = p64.propagation(vp0, rho0, sh, DX, DX, DT, NT, PML, FS, ITER["freq"], 2.0, 1, 1, obs=obs)
+
+    def rel(a, b):
+        a, b = np.asarray(a, np.float64), np.asarray(b, np.float64)
+        return float(np.linalg.norm(a - b) / max(np.linalg.norm(b), 1e-300))
+    return {"seismogram_rel_l2": rel(obs[0], o64[0]), "gradient_rel_l2": rel(g32, g64),
+            "reference": "FP64 build of the same algorithm (oracle restatement compiled with double)",
+            "sample": f"shot {sh[0].shotID} of the survey, nt {NT}; gradient of the starting model with the "
+                      "FP32 observed data", "tolerances": {"seismogram": 1e-5, "gradient": 1e-4}}
+
+
 def step_case(nshot, nt):
     """A short batched forward on the survey model (the step kernel's launch shape at full size)
     for profilers: `ncu ... python bench.py --step-case 60 40`."""
@@ -570,6 +631,28 @@ def step_case(nshot, nt):
     ctx.run(0, path=E.PATH_BATCHED)
     st = ctx.stats()
     print(f"step case: {nshot} shots, {nt} steps, {st['kernel_launches']} launches, {st['ms']:.2f} ms", flush=True)
+    ctx.close()
+
+
+def grad_case(nshot, nt):
+    """A short batched gradient on the survey model for profilers: the forward pass (nt launches of
+    the step kernel) is followed by the adjoint pass, whose launches hold a replay step and an
+    adjoint step each (`ncu -k regex:k_tile -s <nt + 5> ...` captures those)."""
+    from fwiedu import engine as E
+    from fwiedu import models as M
+    vp = M.layered_model(NZ, NX, seed=0)
+    vp0 = M.smooth_model(vp, 15.0)
+    src = M.ricker(nt, DT, 10.0, 0.15)
+    sv = M.line_survey(NZ, NX, DX, DX, DT, nt, nshot, src, spacing_cells=max(1, (NX - 20) // nshot), first_cell=10)
+    shots = M.survey_shots(sv)
+    ctx = E.Context(0)
+    ctx.set_model(vp0, M.gardner(vp0), DX, DX, DT, nt, PML, FS)
+    ctx.set_shots(shots)
+    ctx.set_observed([np.zeros((len(s.igx), s.ns), np.float32) for s in shots])
+    ctx.run(1, 10.0, 2, 1, E.PATH_BATCHED)
+    st = ctx.stats()
+    print(f"grad case: {nshot} shots, {nt} steps, {st['kernel_launches']} launches, {st['ms']:.2f} ms, "
+          f"passes {ctx.pass_stats()}", flush=True)
     ctx.close()
 
 
@@ -590,10 +673,14 @@ def main():
                     help="gradient passes over three surveys of different grids through the serving loop (own line)")
     ap.add_argument("--step-case", nargs=2, type=int, metavar=("SHOTS", "NT"),
                     help="profiling case: one batched forward of SHOTS shots of the survey for NT steps, no JSON line")
+    ap.add_argument("--grad-case", nargs=2, type=int, metavar=("SHOTS", "NT"),
+                    help="profiling case: one batched gradient of SHOTS shots for NT steps, no JSON line")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
     if args.step_case:
         return step_case(*args.step_case)
+    if args.grad_case:
+        return grad_case(*args.grad_case)
     if args.uneven_batch:
         return print(json.dumps(uneven_batch()), flush=True)
     if args.large_survey:
@@ -665,6 +752,7 @@ def main():
         dev_s = float(t.item())
     value = NSHOT * world * args.steps / dev_s
 
+    roof_adj = adjoint_roofline(ctx, E, peaks) if not sharded else None
     plain = plain_path(E, local, vp, rho, vp0, rho0, shots, obs)
     plain_sgps = plain["shot_gradients_per_s"]
 
@@ -715,6 +803,13 @@ def main():
         large["sample"] = (f"{LARGE_SAMPLE} of the 100 shots of the 1201x4001 survey (one wave); "
                            "python bench.py --large-survey runs all 100 in waves")
 
+    err64 = None
+    if rank == 0 and world == 1 and not args.no_cpu:
+        try:
+            err64 = fp64_error(E, vp, rho, vp0, rho0, shots, local)
+        except Exception as ex:  # a reported statement, never required
+            err64 = {"unavailable": str(ex)}
+
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
         try:
@@ -746,7 +841,8 @@ def main():
                                             "one-shot launches already fill most of the GPU, so batching adds "
                                             "occupancy and shared coefficient reads, not an order of magnitude"),
                 "uneven_batch": uneven, "large_survey": large,
-                "wall_s": wall, "gpu_launches": launches, "roofline": roof, "cpu_baseline": cpu, "e2e": e2e,
+                "wall_s": wall, "gpu_launches": launches, "roofline": roof, "roofline_adjoint": roof_adj,
+                "fp64_error": err64, "cpu_baseline": cpu, "e2e": e2e,
                 "serving": serve,
                 "clocks": clk.summary()}
         print(json.dumps(line), flush=True)

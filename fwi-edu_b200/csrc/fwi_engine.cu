@@ -173,6 +173,15 @@ struct fwi_ctx {
         bool warned = false;
     } dump;
     bool snapping = false;  // the launches being issued belong to a pass that writes snapshots
+    // device time of the step-kernel passes of the last run, per pass kind (0 forward of a
+    // gradient or modeling run, 1 adjoint pass with its replay): event pairs around every
+    // program launch, read when the run ends
+    struct PassTimer {
+        std::vector<std::pair<cudaEvent_t, cudaEvent_t>> ev;
+        size_t used = 0;
+        double ms = 0.0;
+        long long launches = 0;
+    } pass[2];
 };
 
 // Device memory comes from the stream-ordered allocator on the context's stream: a context
@@ -259,6 +268,11 @@ extern "C" int fwi_ctx_destroy(fwi_ctx *c)
     c->sizes.clear();
     cudaStreamSynchronize(c->stream);
     cudaEventDestroy(c->ev0); cudaEventDestroy(c->ev1);
+    for (auto &t : c->pass)
+        for (auto &e : t.ev) {
+            cudaEventDestroy(e.first);
+            cudaEventDestroy(e.second);
+        }
     cudaStreamDestroy(c->stream);
     delete c;
     return FWI_OK;
@@ -1200,6 +1214,33 @@ extern "C" int fwi_ctx_set_verbose(fwi_ctx *c, int verbose, int iter, int shot_i
     return FWI_OK;
 }
 
+// ---------------------------------------------------------------- bounded-wait self-test
+// One block waits on an mbarrier phase that nothing completes, with the step kernel's bounded
+// wait: it must give up after limit_ns, set the context's error word and return, so that the
+// host reports FWI_ERR_CUDA and the context stays usable.  No copy, fault or trap is involved.
+static __global__ void k_wait_probe(int *err, unsigned long long limit_ns)
+{
+    __shared__ __align__(8) unsigned long long bar;
+    if (threadIdx.x == 0) {
+        mbar_init(smem_u32(&bar), 1);
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    __syncthreads();
+    const bool ok = mbar_wait(smem_u32(&bar), 0, limit_ns);
+    if (!__all_sync(0xffffffffu, ok) && (threadIdx.x & 31) == 0) atomicExch(err, 1);
+}
+
+extern "C" int fwi_ctx_selftest_wait(fwi_ctx *c, int limit_ms)
+{
+    if (!c) return fail(FWI_ERR_ARG, "NULL context");
+    if (limit_ms < 1 || limit_ms > 2000) return fail(FWI_ERR_ARG, "limit_ms %d outside [1, 2000]", limit_ms);
+    CK(cudaSetDevice(c->device));
+    k_wait_probe<<<1, 64, 0, c->stream>>>(c->d_err, (unsigned long long)limit_ms * 1000000ull);
+    CK(cudaGetLastError());
+    CK(cudaStreamSynchronize(c->stream));
+    return check_kernel_error(c);
+}
+
 static int upload_descs(fwi_ctx *c, const std::vector<ShotDesc> &v)
 {
     if ((int)v.size() > c->desc_cap) {
@@ -1622,11 +1663,6 @@ static int adj_init(fwi_ctx *c, const std::vector<ShotRun *> &rs, int shot_base)
 static int run_program(fwi_ctx *c, const std::string &key, const Program *prog, int shot_base, int nshot,
                        const ShotRun *r0, bool batched)
 {
-    const char *ke = getenv("FWI_KERNEL");
-    const bool tile_kernel = !(ke && strcmp(ke, "step") == 0);
-    if (c->tune && tile_kernel && !getenv("FWI_TX") && !getenv("FWI_NST") && !getenv("FWI_CHUNK") && !getenv("FWI_GPT") &&
-        !getenv("FWI_OCC"))
-        TRY(autotune(c, shot_base, nshot, r0, batched));
     if (c->dump.verbose > 1) {
         // snapshots: direct launches with a copy-out after every snapshot step
         c->snapping = true;
@@ -1660,13 +1696,39 @@ static int run_program(fwi_ctx *c, const std::string &key, const Program *prog, 
     return FWI_OK;
 }
 
+// run_program between a pair of events of the pass kind's timer; the autotuner, which times
+// launch shapes before a new shape's first pass, runs before the first event
+static int timed_program(fwi_ctx *c, int kind, const std::string &key, const Program *prog, int shot_base,
+                         int nshot, const ShotRun *r0, bool batched)
+{
+    const char *ke = getenv("FWI_KERNEL");
+    const bool tile_kernel = !(ke && strcmp(ke, "step") == 0);
+    if (c->tune && tile_kernel && !getenv("FWI_TX") && !getenv("FWI_NST") && !getenv("FWI_CHUNK") && !getenv("FWI_GPT") &&
+        !getenv("FWI_OCC"))
+        TRY(autotune(c, shot_base, nshot, r0, batched));
+    fwi_ctx::PassTimer &t = c->pass[kind];
+    if (t.used == t.ev.size()) {
+        cudaEvent_t a, b;
+        CK(cudaEventCreate(&a));
+        CK(cudaEventCreate(&b));
+        t.ev.push_back({a, b});
+    }
+    const long long l0 = c->launches;
+    auto &e = t.ev[t.used++];
+    CK(cudaEventRecord(e.first, c->stream));
+    TRY(run_program(c, key, prog, shot_base, nshot, r0, batched));
+    CK(cudaEventRecord(e.second, c->stream));
+    t.launches += c->launches - l0;
+    return FWI_OK;
+}
+
 static int run_forward_group(fwi_ctx *c, std::vector<ShotRun *> &rs, int problem, float freq, int filter, bool batched,
                              const std::string &gkey, int shot_base)
 {
     Program *prog;
     TRY(get_program(c, "fwd0", program_forward(c->nt, K_FWD0), &prog));
     for (ShotRun *r : rs) TRY(zero_initial(c, r, false));
-    TRY(run_program(c, "fwd0/" + gkey, prog, shot_base, (int)rs.size(), rs[0], batched));
+    TRY(timed_program(c, 0, "fwd0/" + gkey, prog, shot_base, (int)rs.size(), rs[0], batched));
     if (problem == 2) {
         if (filter < 0 || filter > 2) return fail(FWI_ERR_ARG, "residual filter %d (0 lowpass, 1 bandpass, 2 none)", filter);
         for (ShotRun *r : rs) TRY(prepare_taper(c, r, freq));
@@ -1683,7 +1745,7 @@ static int grad_forward(fwi_ctx *c, std::vector<ShotRun *> &rs, int precondition
     Program *pf;
     TRY(get_program(c, "fwd1", program_forward(c->nt, K_FWD1), &pf));
     for (ShotRun *r : rs) TRY(zero_initial(c, r, true));
-    TRY(run_program(c, "fwd1/" + gkey, pf, shot_base, (int)rs.size(), rs[0], batched));
+    TRY(timed_program(c, 0, "fwd1/" + gkey, pf, shot_base, (int)rs.size(), rs[0], batched));
     if (precondition == 1) TRY(finalize(c, rs, 0));
     return FWI_OK;
 }
@@ -1694,8 +1756,8 @@ static int grad_adjoint(fwi_ctx *c, std::vector<ShotRun *> &rs, bool batched, co
     Program *pa;
     TRY(get_program(c, batched ? "adj/overlap" : "adj/plain", program_adjoint(c->nt, batched), &pa));
     TRY(adj_init(c, rs, shot_base));
-    TRY(run_program(c, std::string(batched ? "adjo/" : "adjp/") + gkey, pa, shot_base, (int)rs.size(), rs[0],
-                    batched));
+    TRY(timed_program(c, 1, std::string(batched ? "adjo/" : "adjp/") + gkey, pa, shot_base, (int)rs.size(), rs[0],
+                      batched));
     TRY(finalize(c, rs, 1));
     return FWI_OK;
 }
@@ -1764,6 +1826,11 @@ extern "C" int fwi_ctx_run(fwi_ctx *c, int problem, float freq, int filter, int 
     const int ns = (int)c->shots.size();
     long long launches0 = c->launches;
     double cells = 0.0;
+    for (auto &t : c->pass) {
+        t.used = 0;
+        t.ms = 0.0;
+        t.launches = 0;
+    }
     CK(cudaEventRecord(c->ev0, c->stream));
     if (batched) {
         // one group per plan geometry: shots sharing a window run in the same launches
@@ -1877,6 +1944,12 @@ extern "C" int fwi_ctx_run(fwi_ctx *c, int problem, float freq, int filter, int 
     TRY(check_kernel_error(c));
     float ms = 0.f;
     CK(cudaEventElapsedTime(&ms, c->ev0, c->ev1));
+    for (auto &t : c->pass)
+        for (size_t k = 0; k < t.used; k++) {
+            float m = 0.f;
+            CK(cudaEventElapsedTime(&m, t.ev[k].first, t.ev[k].second));
+            t.ms += m;
+        }
     for (int i = 0; i < ns; i++) {
         const fwi_shot &s = c->shots[i].s;
         double cellsz = (double)(c->nz + 2 * c->pml) * (s.ix_max - s.ix_min + 1 + 2 * c->pml);
@@ -2034,6 +2107,17 @@ extern "C" int fwi_ctx_stats(fwi_ctx *c, fwi_stats *out)
 {
     if (!c || !out) return fail(FWI_ERR_ARG, "NULL argument");
     *out = c->stats;
+    return FWI_OK;
+}
+
+extern "C" int fwi_ctx_pass_stats(fwi_ctx *c, double *fwd_ms, long long *fwd_launches, double *adj_ms,
+                                  long long *adj_launches)
+{
+    if (!c) return fail(FWI_ERR_ARG, "NULL context");
+    if (fwd_ms) *fwd_ms = c->pass[0].ms;
+    if (fwd_launches) *fwd_launches = c->pass[0].launches;
+    if (adj_ms) *adj_ms = c->pass[1].ms;
+    if (adj_launches) *adj_launches = c->pass[1].launches;
     return FWI_OK;
 }
 

@@ -182,15 +182,15 @@ __device__ __forceinline__ bool mbar_try(unsigned bar, unsigned parity)
                  : "memory");
     return done != 0;
 }
-// waits for the phase of the given parity to complete; false after two seconds (the clock
-// is read only when the first try finds the phase still open)
-__device__ __forceinline__ bool mbar_wait(unsigned bar, unsigned parity)
+// waits for the phase of the given parity to complete; false after limit_ns (two seconds unless
+// given; the clock is read only when the first try finds the phase still open)
+__device__ __forceinline__ bool mbar_wait(unsigned bar, unsigned parity, u64 limit_ns = 2000000000ull)
 {
     if (mbar_try(bar, parity)) return true;
     const u64 t0 = global_ns();
     for (;;) {
         if (mbar_try(bar, parity)) return true;
-        if (global_ns() - t0 > 2000000000ull) return false;
+        if (global_ns() - t0 > limit_ns) return false;
     }
 }
 // a 16-byte shared-memory load at a 32-bit shared address (volatile: never moved above the

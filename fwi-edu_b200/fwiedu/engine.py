@@ -264,6 +264,13 @@ class Context:
         _check(self.L.fwi_ctx_get_model(self.h, _ptr(vp), _ptr(rho)))
         return vp, rho
 
+    def pass_stats(self):
+        """Device time and step launches of the last run's forward and adjoint passes."""
+        fm, am = C.c_double(), C.c_double()
+        fl, al = C.c_longlong(), C.c_longlong()
+        _check(self.L.fwi_ctx_pass_stats(self.h, C.byref(fm), C.byref(fl), C.byref(am), C.byref(al)))
+        return {"fwd_ms": fm.value, "fwd_launches": fl.value, "adj_ms": am.value, "adj_launches": al.value}
+
     def set_verbose(self, verbose, iteration=1, shot_interval=0, snap_interval=0, directory=None):
         """The reference's intermediate files (fwi_ctx_set_verbose): verbose 1 per-shot traces and
         gradients and the stacked gradient of a gradient run, verbose 2 also wavefield snapshots.

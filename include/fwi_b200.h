@@ -197,6 +197,12 @@ typedef struct {
     size_t device_bytes;     /* device memory held by the context */
 } fwi_stats;
 FWI_API int fwi_ctx_stats(fwi_ctx *ctx, fwi_stats *out);
+/* device time and step-kernel launches of the last run's passes: the forward passes (modeling,
+ * or the checkpointing forward of a gradient) and the adjoint passes (each launch a replay step
+ * and an adjoint step of every shot of the group), summed over shot groups and waves; the
+ * autotuner's probes are not included */
+FWI_API int fwi_ctx_pass_stats(fwi_ctx *ctx, double *fwd_ms, long long *fwd_launches, double *adj_ms,
+                               long long *adj_launches);
 
 /* The step kernel's launch shape (tile width 8/16 columns, z-groups per thread, blocks per SM it
  * is compiled for, shared-memory ring depth 2..4 shots, shots per block) is picked by an
@@ -342,6 +348,13 @@ FWI_API int fwi_ctx_get_model(fwi_ctx *ctx, float *vp, float *rho);
  * overlap on the GPU race on it.
  * stream is a cudaStream_t (NULL: the legacy default stream); the call only enqueues work. */
 FWI_API int fwi_smooth2d_noalloc(const float *d_in, float *d_out, int nx, int nz, int rz, int rx, void *stream);
+
+/* Self-test of the failure path of the step kernel's waits (no counterpart in the reference): a
+ * one-block kernel waits, with the step kernel's bounded wait and a limit of limit_ms (1..2000),
+ * on an mbarrier phase that nothing completes; it gives up, sets the context's error word and
+ * returns.  Returns FWI_ERR_CUDA with the message a stalled tile copy produces (the expected
+ * outcome); the context stays usable. */
+FWI_API int fwi_ctx_selftest_wait(fwi_ctx *ctx, int limit_ms);
 
 /* Measurement helper (no counterpart in the reference): the L2 bandwidth figure that bounds the
  * plain one-shot-per-launch path, whose per-shot state stays in L2.  Copies `bytes` between the

@@ -1,0 +1,59 @@
+"""The reference's own front-ends, linked against this library, run the shape of the reference's
+Marmousi-II demo (demo/marm-ii/modeling.sh, fwi.sh): acquisition from a JSON file
+(observation.c:422-532), a 30-cell absorbing layer, nt = 6001, records decimated by
+sampleRate = 2 (so the adjoint sources are interpolated back, common.c:482-582), a 36-cell
+water layer with Gardner density, verbose output, and a multiscale schedule whose first stage
+uses the low-pass residual filter.  Subset: two shots of the demo's acquisition rule and one
+iteration per stage, on a seeded stand-in model of the demo's grid (tests/golden/make_demo.py
+states the run and produced the expected outputs with the reference's own build).
+
+Compared with the reference's outputs: the modeling SU file byte for byte, the set of files
+each front-end writes (the engine's verbose files included), the misfit history, the first
+iteration's gradient and the final model within the FP32 tolerance of the FFT stages
+(1e-4 relative).
+"""
+import hashlib
+import os
+import sys
+
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.join(HERE, "golden"))
+REF = os.path.join(HERE, "..", "oracle", "_ref")
+
+import make_demo as D  # noqa: E402
+
+
+def rel(a, b):
+    a = np.asarray(a, np.float64)
+    b = np.asarray(b, np.float64)
+    return float(np.linalg.norm(a - b) / max(np.linalg.norm(b), 1e-300))
+
+
+def test_demo_front_ends(tmp_path):
+    exes = [os.path.join(REF, f"acoustic2d_{k}_b200.exe") for k in ("modeling", "fwi")]
+    if not all(os.path.exists(e) for e in exes):
+        pytest.skip("front-ends linked against the engine not built (make -C oracle frontends_b200)")
+    want = np.load(os.path.join(HERE, "golden", "demo_marm.npz"))
+    vp, vp0, src, geometry = D.inputs()
+    assert D.digest(vp, vp0, src, geometry) == str(want["inputs_sha256"]), "stand-in inputs changed"
+    paths = D.write_inputs(str(tmp_path), vp, vp0, src, geometry)
+    dm, df = D.run_demo(exes[0], exes[1], str(tmp_path), paths)
+    assert sorted(os.listdir(dm)) == list(want["modeling_files"])
+    su = os.path.join(dm, str(want["su_name"]))
+    assert hashlib.sha256(open(su, "rb").read()).hexdigest() == str(want["su_sha256"]), "modeling SU differs"
+    files = sorted(os.listdir(df))
+    assert files == list(want["fwi_files"])
+
+    def load(prefix):
+        return np.fromfile(os.path.join(df, [f for f in files if f.startswith(prefix)][0]), np.float32)
+
+    obj = load("objective_function_")
+    assert obj.shape == want["objective"].shape
+    assert np.all(np.abs(obj - want["objective"]) <= 1e-4 * np.abs(want["objective"]))
+    assert rel(load("grad_iter001_"), want["grad_iter001"]) <= 1e-4
+    assert rel(load("vp_inversion_"), want["vp_inversion"]) <= 1e-4

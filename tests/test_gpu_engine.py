@@ -214,3 +214,23 @@ def test_fwi_iteration_matches_oracle(port32):
     assert np.float32(r["scalar"]) == np.float32(scalar)
     assert abs(r["steplen"] - steplen) <= 1e-6 * abs(steplen)
     assert rel(vp_g, vp2) <= 1e-6 and rel(rho_g, rho2) <= 1e-6
+
+
+def test_bounded_wait_gives_up_and_context_survives():
+    """The step kernel's mbarrier waits are bounded: a wait on a phase that nothing completes gives
+    up after its limit, the kernel sets the error word and returns, the host reports FWI_ERR_CUDA,
+    and the same context then runs a golden case bit for bit (no fault, no hang, no reset)."""
+    c = Case("fs1_small")
+    ctx = E.Context(0)
+    try:
+        L = E.lib()
+        assert L.fwi_ctx_selftest_wait(ctx.h, 50) == E.FWI_ERR_CUDA
+        assert b"did not complete" in L.fwi_last_error()
+        assert L.fwi_ctx_selftest_wait(ctx.h, 0) == E.FWI_ERR_ARG
+        ctx.set_model(c.vp, c.rho, c.dx, c.dx, c.dt, c.nt, c.pml, c.fs)
+        ctx.set_shots(c.shots)
+        ctx.run(0, path=E.PATH_BATCHED)
+        for i in range(c.nshot):
+            assert np.array_equal(ctx.traces(i), c.obs[i])
+    finally:
+        ctx.close()
