@@ -309,15 +309,13 @@ class ContextE2E:
 SERVE_GRIDS = [(221, 601, 12.5, 0.001), (301, 901, 12.5, 0.001), (401, 1201, 10.0, 0.0008), (601, 2001, 10.0, 0.0008)]
 
 
-def serving(E, M, nreq, rate, seed=0, max_active=4):
-    """The serving loop under a Poisson stream of mixed requests (the serving configuration of the
-    survey: 70 % one-shot modeling, 30 % 8-shot gradients, grids from four sizes, nt uniform in
-    2001..6001), submitted as they arrive; latency from submission to completion."""
+def serving(E, M, nreq, rate, seed=0, max_active=32):
+    """The serving loop under a Poisson stream of mixed requests (the serving configuration: 70 %
+    one-shot modeling, 30 % 8-shot gradients, grids drawn from four sizes, nt uniform in
+    2001..6001, each request's model generated from its own seed), submitted as they arrive;
+    latency from submission to completion.  Requests in flight share the step launches
+    (continuous batching)."""
     rng = np.random.default_rng(seed)
-    models = {}
-    for g, (nz, nx, dx, dt) in enumerate(SERVE_GRIDS):
-        vp = M.layered_model(nz, nx, seed=100 + g, water_rows=WATER)
-        models[g] = (vp, M.gardner(vp, water_rows=WATER))
     plan = []
     t = 0.0
     for i in range(nreq):
@@ -327,11 +325,12 @@ def serving(E, M, nreq, rate, seed=0, max_active=4):
         nt = int(rng.integers(2001, 6002))
         grad = rng.random() < 0.3
         nshot = 8 if grad else 1
+        vp = M.layered_model(nz, nx, seed=1000 * (seed + 1) + i, water_rows=WATER)
+        rho = M.gardner(vp, water_rows=WATER)
         src = M.ricker(nt, dt, 10.0, 0.15)
         first = int(rng.integers(0, nx - 8 * 20))
         sv = M.line_survey(nz, nx, dx, dx, dt, nt, nshot, src, spacing_cells=20, first_cell=first)
         shots = M.survey_shots(sv)
-        vp, rho = models[g]
         kw = dict(vp=vp, rho=rho, dx=dx, dz=dx, dt=dt, nt=nt, pml=PML, fs=FS, shots=shots)
         if grad:
             zero = np.zeros((len(shots[0].igx), shots[0].ns), np.float32)  # one host array for all 8 shots
@@ -354,15 +353,26 @@ def serving(E, M, nreq, rate, seed=0, max_active=4):
     ngrad = sum(p[4] for p in plan if p[3])
     nmod = sum(p[4] for p in plan if not p[3])
     return {"requests": nreq, "arrival_rate_per_s": rate, "completed": rep["completed"], "failed": rep["failed"],
-            "mix": "70% 1-shot modeling, 30% 8-shot gradient; grids 221x601@12.5m, 301x901@12.5m, 401x1201@10m, "
-                   "601x2001@10m; nt uniform 2001..6001; Poisson arrivals",
             "latency_ms": {"p50": rep["p50_ms"], "p99": rep["p99_ms"], "max": rep["max_ms"]},
             "queue_ms": {"p50": rep["p50_queue_ms"], "p99": rep["p99_queue_ms"]},
             "service_ms": {"p50": float(np.percentile([x["run_ms"] for x in ok], 50)) if ok else None,
                            "p99": float(np.percentile([x["run_ms"] for x in ok], 99)) if ok else None},
-            "requests_per_s": len(ok) / wall, "shot_gradients_per_s": ngrad / wall, "shots_modeled_per_s": nmod / wall,
+            "requests_per_s": len(ok) / wall, "shots_per_s": (ngrad + nmod) / wall,
+            "shot_gradients_per_s": ngrad / wall, "shots_modeled_per_s": nmod / wall,
             "gcells_per_s": rep["cell_updates"] / wall / 1e9, "wall_s": wall, "max_active": rep["max_active"],
             "peak_active": rep["peak_active"], "peak_admitted_bytes": rep["peak_bytes"], "budget_bytes": rep["budget"]}
+
+
+SERVE_RATES = (10.0, 100.0, 500.0)
+
+
+def serving_sweep(E, M, nreq, rates=SERVE_RATES):
+    """The serving configuration at several Poisson arrival rates (a stated fraction of its 2000
+    requests per rate; `--serve-requests` sets it)."""
+    runs = [serving(E, M, nreq, r, seed=k) for k, r in enumerate(rates)]
+    return {"mix": "70% 1-shot modeling, 30% 8-shot gradient; grids 221x601@12.5m, 301x901@12.5m, 401x1201@10m, "
+                   "601x2001@10m; nt uniform 2001..6001; model per request from its own seed; Poisson arrivals",
+            "requests_per_rate": nreq, "of": 2000, "rates": runs}
 
 
 # uneven-size gradient batch: (shots, nz, nx, d, dt, nt, Ricker peak)
@@ -665,8 +675,8 @@ def main():
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline sample")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-extra", action="store_true", help="skip the uneven-batch and large-grid sub-measurements")
-    ap.add_argument("--serve-requests", type=int, default=40, help="requests of the serving measurement (0: skip)")
-    ap.add_argument("--serve-rate", type=float, default=20.0, help="Poisson arrival rate of the serving measurement")
+    ap.add_argument("--serve-requests", type=int, default=100,
+                    help="requests per arrival rate of the serving measurement (0: skip)")
     ap.add_argument("--large-survey", action="store_true",
                     help="one gradient over 100 shots on the 1201 x 4001 grid, run in waves (own line)")
     ap.add_argument("--uneven-batch", action="store_true",
@@ -792,7 +802,7 @@ def main():
     serve = None
     if args.serve_requests > 0 and not sharded:
         from fwiedu import models as M
-        serve = serving(E, M, args.serve_requests, args.serve_rate)
+        serve = serving_sweep(E, M, args.serve_requests)
 
     uneven = large = None
     if rank == 0 and world == 1 and not args.no_extra:

@@ -679,9 +679,9 @@ static int prepare_taper(fwi_ctx *c, ShotRun *r, float freq)
     std::vector<float> a(Lt + 1), b(Lr + 1);
     if (Lt > 0) fwi_taper_coefs(Lt, a.data());
     if (Lr > 0) fwi_taper_coefs(Lr, b.data());
+    // pageable sources: staged before the calls return
     CK(cudaMemcpyAsync(r->d_tct, a.data(), (Lt + 1) * 4, cudaMemcpyHostToDevice, c->stream));
     CK(cudaMemcpyAsync(r->d_tcr, b.data(), (Lr + 1) * 4, cudaMemcpyHostToDevice, c->stream));
-    CK(cudaStreamSynchronize(c->stream));
     return FWI_OK;
 }
 
@@ -1267,7 +1267,9 @@ static int scratch(fwi_ctx *c, size_t bytes, void **out)
     return FWI_OK;
 }
 
-// small descriptor arrays go through a pinned staging copy on the stream
+// small descriptor arrays into the scratch area, ordered on the stream: a copy from pageable host
+// memory is staged before cudaMemcpyAsync returns (the host vector may go), and the kernels that
+// read the previous contents of the area run before the copy on the same stream
 template <class T>
 static int put(fwi_ctx *c, const std::vector<T> &v, T **dev, size_t offset_bytes)
 {
@@ -1275,7 +1277,6 @@ static int put(fwi_ctx *c, const std::vector<T> &v, T **dev, size_t offset_bytes
     TRY(scratch(c, offset_bytes + v.size() * sizeof(T) + 256, &base));
     *dev = (T *)((char *)base + offset_bytes);
     CK(cudaMemcpyAsync(*dev, v.data(), v.size() * sizeof(T), cudaMemcpyHostToDevice, c->stream));
-    CK(cudaStreamSynchronize(c->stream));
     return FWI_OK;
 }
 
@@ -1285,8 +1286,10 @@ static int ensure_red(fwi_ctx *c)
     return FWI_OK;
 }
 
-// FP64 sums of several arrays: results in out_host (2 per descriptor)
-static int reduce(fwi_ctx *c, std::vector<SumDesc> sd, std::vector<double> &out_host, double **out_dev = nullptr)
+// FP64 sums of several arrays: results on the device (2 per descriptor, *out_dev) and, unless
+// to_host is false, in out_host (a host round trip)
+static int reduce(fwi_ctx *c, std::vector<SumDesc> sd, std::vector<double> &out_host, double **out_dev = nullptr,
+                  bool to_host = true)
 {
     TRY(ensure_red(c));
     const int NP = 592;  // partials per array: 4 per SM
@@ -1301,6 +1304,7 @@ static int reduce(fwi_ctx *c, std::vector<SumDesc> sd, std::vector<double> &out_
     c->launches += 2;
     CK(cudaGetLastError());
     if (out_dev) *out_dev = res;
+    if (!to_host) return FWI_OK;
     out_host.resize(2 * nd);
     CK(cudaMemcpyAsync(out_host.data(), res, 2 * nd * 8, cudaMemcpyDeviceToHost, c->stream));
     CK(cudaStreamSynchronize(c->stream));
@@ -1511,7 +1515,7 @@ static int shot_precondition(fwi_ctx *c, const std::vector<ShotRun *> &rs)
     double *res;
     for (size_t i0 = 0; i0 < sd.size(); i0 += 64) {
         std::vector<SumDesc> part(sd.begin() + i0, sd.begin() + std::min(sd.size(), i0 + 64));
-        TRY(reduce(c, part, h, &res));
+        TRY(reduce(c, part, h, &res, false));
         std::vector<PrecDesc> pd;
         for (size_t i = 0; i < part.size(); i++) {
             ShotRun *r = rs[i0 + i];
@@ -1527,7 +1531,6 @@ static int shot_precondition(fwi_ctx *c, const std::vector<ShotRun *> &rs)
         k_shot_precondition<<<dim3(148, (unsigned)pd.size()), 256, 0, c->stream>>>(d);
         c->launches++;
         CK(cudaGetLastError());
-        CK(cudaStreamSynchronize(c->stream));
     }
     return FWI_OK;
 }
@@ -1609,7 +1612,7 @@ static int stack_and_precondition(fwi_ctx *c, const std::vector<ShotRun *> &rs, 
         s.op = 2;
         std::vector<double> h;
         double *res;
-        TRY(reduce(c, {s}, h, &res));
+        TRY(reduce(c, {s}, h, &res, false));
         k_global_precondition<<<592, 256, 0, c->stream>>>(c->d_grad, c->d_prec, m, res, 0.005f);
         c->launches++;
     }
@@ -2406,3 +2409,6 @@ extern "C" int fwi_ctx_fwi_iteration(fwi_ctx *c, const fwi_iter_params *p, fwi_i
     out->kernel_launches = c->launches - l0;
     return FWI_OK;
 }
+
+// ------------------------------------------------------------------ continuous batching
+#include "fwi_exec.cuh"

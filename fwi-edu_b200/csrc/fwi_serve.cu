@@ -1,19 +1,24 @@
 // fwi_serve.cu -- the request loop: modeling and gradient requests of any grid size, admitted
-// by device-memory footprint and run concurrently on one GPU.
+// by device-memory footprint and batched continuously on one GPU.
 //
 // Requests arrive through fwi_server_submit from any host thread.  The server keeps them in
-// arrival order and admits the oldest one as soon as a worker is free and its footprint
-// (fwi_estimate_bytes) fits into the budget left by the requests already running; requests
-// that arrive while others are on the GPU are therefore admitted as slots and memory free up
-// (continuous admission, not a queue drained one at a time).  Every worker owns a CUDA stream
-// through its own engine context, so admitted requests overlap on the device; the engine's
-// allocations are stream-ordered, so one request growing or releasing its state never stalls
-// the others.  Each request's result depends on its inputs only (the engine is deterministic
-// and contexts share nothing), so it is the same alone and in any mix.
+// arrival order and admits the oldest one as soon as fewer than `max_active` requests are in
+// flight and its footprint (fwi_estimate_bytes) fits into the budget left by the requests
+// already admitted (strictly first come, first served: a request that does not fit waits at
+// the head, so none starves; one larger than the whole budget is rejected at submission).
 //
-// Admission is strictly first come, first served: a request that does not fit waits at the
-// head until enough memory is released (no later request overtakes it, so none starves).  A
-// request larger than the whole budget is rejected at submission.
+// An admitted request goes through three stages, each on its own threads:
+//  * set-up (two threads): a context of its own, the model's coefficients on the host, shots
+//    and observed data uploaded on the context's stream, the run's state allocated -- then the
+//    run is added to the server's executor (fwi_exec_add);
+//  * the batch (one thread): the executor's step launches advance every run in the batch at
+//    once, one program item each (continuous batching: a run set up while others are on the
+//    GPU joins at the next launch, and a modeling request of one shot shares every launch with
+//    the runs around it instead of filling the GPU with one small grid);
+//  * hand-back (one thread): results copied into the caller's buffers on the context's own
+//    stream, the context released, the request's memory returned to the budget.
+// Each request's result depends on its inputs only (the executor's runs are bit-identical to
+// their runs alone), so it is the same alone and in any mix.
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -37,6 +42,7 @@ using Clock = std::chrono::steady_clock;
 struct Job {
     long long id = 0;
     fwi_request req{};
+    fwi_ctx *ctx = nullptr;
     size_t bytes = 0;
     int state = FWI_REQ_QUEUED;
     int status = FWI_OK;
@@ -64,14 +70,19 @@ struct fwi_server {
     size_t budget = 0;
     int max_active = 1;
     std::mutex mu;
-    std::condition_variable cv_work, cv_done;
-    std::deque<Job *> queue;
+    std::condition_variable cv_work, cv_done, cv_batch, cv_back;
+    std::deque<Job *> queue;          // submitted, not admitted
+    std::deque<Job *> to_setup;       // admitted, waiting for a set-up thread
+    std::vector<Job *> in_batch;      // added to the executor
+    std::deque<Job *> to_hand_back;   // handed back by the executor
     std::map<long long, Job *> jobs;
     std::vector<std::thread> workers;
+    fwi_exec *ex = nullptr;
+    int setting_up = 0;
     size_t in_use = 0, peak_bytes = 0;
     int active = 0, peak_active = 0;
     long long next_id = 1, submitted = 0, completed = 0, failed = 0, rejected = 0;
-    bool stop = false, any = false;
+    bool stop = false, any = false, batch_done = false;
     Clock::time_point t_first, t_last;
     std::vector<double> lat_ms, queue_ms;
     double cell_updates = 0.0, shots_modeled = 0.0, shot_gradients = 0.0;
@@ -79,21 +90,26 @@ struct fwi_server {
 
 namespace {
 
-// one request on a fresh engine context of this worker's thread
-void run_job(fwi_server *s, Job *j)
+// stage 1: a context for the request, its inputs, and the run added to the executor
+int set_up(fwi_server *s, Job *j)
 {
     const fwi_request &r = j->req;
-    fwi_ctx *c = nullptr;
-    int rc = fwi_ctx_create(&c, s->device, 0);
-    if (rc == FWI_OK) rc = fwi_ctx_set_graphs(c, 0);  // one-off launch sequences: capturing them does not pay
+    int rc = fwi_ctx_create(&j->ctx, s->device, 0);
     if (rc == FWI_OK)
-        rc = fwi_ctx_set_model(c, r.vp, r.rho, r.nz, r.nx, r.dx, r.dz, r.dt, r.nt, r.pml, r.fs);
-    if (rc == FWI_OK) rc = fwi_ctx_set_shots(c, r.shots, r.nshot);
-    if (rc == FWI_OK && r.kind == FWI_REQ_GRADIENT) rc = fwi_ctx_set_observed(c, r.obs);
-    if (rc == FWI_OK) {
-        const int problem = r.kind == FWI_REQ_GRADIENT ? 1 : 0;
-        rc = fwi_ctx_run(c, problem, r.freq, r.filter, r.precondition, FWI_PATH_BATCHED);
-    }
+        rc = fwi_ctx_set_model(j->ctx, r.vp, r.rho, r.nz, r.nx, r.dx, r.dz, r.dt, r.nt, r.pml, r.fs);
+    if (rc == FWI_OK) rc = fwi_ctx_set_shots(j->ctx, r.shots, r.nshot);
+    if (rc == FWI_OK && r.kind == FWI_REQ_GRADIENT) rc = fwi_ctx_set_observed(j->ctx, r.obs);
+    if (rc == FWI_OK)
+        rc = fwi_exec_add(s->ex, j->ctx, r.kind == FWI_REQ_GRADIENT ? 1 : 0, r.freq, r.filter, r.precondition);
+    return rc;
+}
+
+// stage 3: results into the caller's buffers (the context's stream is ordered after the run)
+int hand_back(Job *j)
+{
+    const fwi_request &r = j->req;
+    fwi_ctx *c = j->ctx;
+    int rc = j->status;
     if (rc == FWI_OK && r.traces)
         for (int i = 0; i < r.nshot && rc == FWI_OK; i++)
             if (r.traces[i]) rc = fwi_ctx_get_traces(c, i, r.traces[i]);
@@ -105,22 +121,43 @@ void run_job(fwi_server *s, Job *j)
         fwi_stats st;
         if (fwi_ctx_stats(c, &st) == FWI_OK) j->cell_updates = st.cell_updates;
     }
-    if (rc != FWI_OK) j->error = fwi_last_error();
-    if (c) fwi_ctx_destroy(c);
-    j->status = rc;
+    return rc;
 }
 
-void worker_main(fwi_server *s)
+// the request leaves the server (any stage): context released, memory and slot returned
+void finish(fwi_server *s, Job *j, int rc, std::unique_lock<std::mutex> &lk)
 {
-    cudaSetDevice(s->device);
-    std::unique_lock<std::mutex> lk(s->mu);
-    for (;;) {
-        // admit the oldest request once it fits next to the running ones
-        s->cv_work.wait(lk, [&] {
-            return (!s->queue.empty() && s->in_use + s->queue.front()->bytes <= s->budget) ||
-                   (s->stop && s->queue.empty());
-        });
-        if (s->queue.empty()) return;  // shutting down, nothing left to run
+    if (rc != FWI_OK && j->error.empty()) j->error = fwi_last_error();
+    fwi_ctx *c = j->ctx;
+    j->ctx = nullptr;
+    lk.unlock();
+    if (c) fwi_ctx_destroy(c);
+    lk.lock();
+    j->status = rc;
+    j->t_end = Clock::now();
+    j->state = rc == FWI_OK ? FWI_REQ_DONE : FWI_REQ_FAILED;
+    s->in_use -= j->bytes;
+    s->active--;
+    s->t_last = j->t_end;
+    if (rc == FWI_OK) {
+        s->completed++;
+        s->lat_ms.push_back(ms(j->t_submit, j->t_end));
+        s->queue_ms.push_back(ms(j->t_submit, j->t_start));
+        s->cell_updates += j->cell_updates;
+        if (j->req.kind == FWI_REQ_GRADIENT) s->shot_gradients += j->req.nshot;
+        else s->shots_modeled += j->req.nshot;
+    } else {
+        s->failed++;
+    }
+    s->cv_done.notify_all();
+    s->cv_work.notify_all();   // memory and a slot were released
+    s->cv_batch.notify_all();  // the batch thread may be waiting to shut down
+}
+
+// admission: the oldest request, once a slot is free and its footprint fits (caller holds mu)
+void admit(fwi_server *s)
+{
+    while (!s->queue.empty() && s->active < s->max_active && s->in_use + s->queue.front()->bytes <= s->budget) {
         Job *j = s->queue.front();
         s->queue.pop_front();
         s->in_use += j->bytes;
@@ -129,26 +166,86 @@ void worker_main(fwi_server *s)
         s->peak_active = std::max(s->peak_active, s->active);
         j->state = FWI_REQ_RUNNING;
         j->t_start = Clock::now();
+        s->to_setup.push_back(j);
+    }
+}
+
+void setup_main(fwi_server *s)
+{
+    cudaSetDevice(s->device);
+    std::unique_lock<std::mutex> lk(s->mu);
+    for (;;) {
+        admit(s);
+        s->cv_work.wait(lk, [&] {
+            admit(s);
+            return !s->to_setup.empty() || (s->stop && s->queue.empty());
+        });
+        if (s->to_setup.empty()) return;  // shutting down, nothing left to set up
+        Job *j = s->to_setup.front();
+        s->to_setup.pop_front();
+        s->setting_up++;
         lk.unlock();
-        run_job(s, j);
+        const int rc = set_up(s, j);
+        if (rc != FWI_OK) j->error = fwi_last_error();
         lk.lock();
-        j->t_end = Clock::now();
-        j->state = j->status == FWI_OK ? FWI_REQ_DONE : FWI_REQ_FAILED;
-        s->in_use -= j->bytes;
-        s->active--;
-        s->t_last = j->t_end;
-        if (j->status == FWI_OK) {
-            s->completed++;
-            s->lat_ms.push_back(ms(j->t_submit, j->t_end));
-            s->queue_ms.push_back(ms(j->t_submit, j->t_start));
-            s->cell_updates += j->cell_updates;
-            if (j->req.kind == FWI_REQ_GRADIENT) s->shot_gradients += j->req.nshot;
-            else s->shots_modeled += j->req.nshot;
+        s->setting_up--;
+        if (rc == FWI_OK) {
+            s->in_batch.push_back(j);
+            s->cv_batch.notify_all();
         } else {
-            s->failed++;
+            finish(s, j, rc, lk);
         }
-        s->cv_done.notify_all();
-        s->cv_work.notify_all();  // memory and a slot were released
+    }
+}
+
+// stage 2: the executor's launches while any run is in the batch; runs it hands back move on
+void batch_main(fwi_server *s)
+{
+    cudaSetDevice(s->device);
+    std::unique_lock<std::mutex> lk(s->mu);
+    for (;;) {
+        s->cv_batch.wait(lk, [&] {
+            return !s->in_batch.empty() || (s->stop && s->queue.empty() && s->to_setup.empty() && s->setting_up == 0);
+        });
+        if (s->in_batch.empty()) {
+            s->batch_done = true;
+            s->cv_back.notify_all();
+            return;
+        }
+        lk.unlock();
+        int active = 0;
+        const int rc = fwi_exec_step(s->ex, 16, &active);
+        lk.lock();
+        for (size_t i = 0; i < s->in_batch.size();) {
+            Job *j = s->in_batch[i];
+            int done = 0, st = FWI_OK;
+            fwi_exec_poll(s->ex, j->ctx, &done, &st);
+            if (!done && rc != FWI_OK && active == 0) done = 1, st = rc;  // the executor failed its runs
+            if (done) {
+                j->status = st;
+                s->to_hand_back.push_back(j);
+                s->in_batch.erase(s->in_batch.begin() + i);
+                s->cv_back.notify_all();
+            } else {
+                i++;
+            }
+        }
+    }
+}
+
+void back_main(fwi_server *s)
+{
+    cudaSetDevice(s->device);
+    std::unique_lock<std::mutex> lk(s->mu);
+    for (;;) {
+        s->cv_back.wait(lk, [&] { return !s->to_hand_back.empty() || s->batch_done; });
+        if (s->to_hand_back.empty()) return;
+        Job *j = s->to_hand_back.front();
+        s->to_hand_back.pop_front();
+        lk.unlock();
+        const int rc = hand_back(j);
+        lk.lock();
+        finish(s, j, rc, lk);
     }
 }
 
@@ -173,7 +270,13 @@ extern "C" int fwi_server_create(fwi_server **out, int device, size_t hbm_budget
         uint64_t keep = (uint64_t)s->budget;
         cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep);
     }
-    for (int i = 0; i < max_active; i++) s->workers.emplace_back(worker_main, s);
+    if (fwi_exec_create(&s->ex, device) != FWI_OK) {
+        delete s;
+        return FWI_ERR_CUDA;
+    }
+    for (int i = 0; i < 2; i++) s->workers.emplace_back(setup_main, s);
+    s->workers.emplace_back(batch_main, s);
+    s->workers.emplace_back(back_main, s);
     *out = s;
     return FWI_OK;
 }
@@ -275,7 +378,9 @@ extern "C" int fwi_server_destroy(fwi_server *s)
         s->stop = true;  // the workers finish every request already submitted, then exit
     }
     s->cv_work.notify_all();
+    s->cv_batch.notify_all();
     for (auto &t : s->workers) t.join();
+    fwi_exec_destroy(s->ex);
     for (auto &kv : s->jobs) delete kv.second;
     delete s;
     return FWI_OK;

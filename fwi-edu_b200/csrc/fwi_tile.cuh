@@ -258,7 +258,7 @@ struct TileGeom {
     static constexpr int smem(int nst) { return ST_OFF + nst * STAGE; }
 };
 // grid: x = column tile (plus one receiver-sampling index), y = 2 * shot chunk + program
-// item, z = tile of TG z-groups.  block = (TG / GPT) x (TX + 32 / (TG / GPT)) threads: rows
+// item (passed as `by`), z = tile of TG z-groups.  block = (TG / GPT) x (TX + 32 / (TG / GPT)) threads: rows
 // 0..TX-1 are the consumers (GPT consecutive z-groups of one column each), the remaining rows
 // form the producer warp.
 // Dynamic shared memory: TileGeom<TX>::smem(NST).
@@ -272,7 +272,7 @@ struct TileGeom {
 template <int TX, int NST, int MATH, int GPT, int MINB>
 __device__ __forceinline__ void tile_body(const CUtensorMap &tm_p1, const CUtensorMap &tm_p0, const CUtensorMap &tm_cf,
                                           const ShotDesc *__restrict__ shots, const int4 *__restrict__ prog, int L,
-                                          int shot_base, int nshot, int chunk, int *err)
+                                          int shot_base, int nshot, int chunk, int *err, int by)
 {
     using Geo = TileGeom<TX>;
     constexpr int NL = TG / GPT;  // consumer lanes per column
@@ -290,10 +290,10 @@ __device__ __forceinline__ void tile_body(const CUtensorMap &tm_p1, const CUtens
 
     grid_dep_launch();  // the next step may begin its set-up once every block of this one runs
     const int4 pw = prog[L];
-    const int kind = (blockIdx.y & 1) ? pw.z : pw.x;
-    const int it = (blockIdx.y & 1) ? pw.w : pw.y;
+    const int kind = (by & 1) ? pw.z : pw.x;
+    const int it = (by & 1) ? pw.w : pw.y;
     if (kind == K_NONE) return;
-    const int cb = shot_base + (blockIdx.y >> 1) * chunk;
+    const int cb = shot_base + (by >> 1) * chunk;
     const int n = min(chunk, shot_base + nshot - cb);
     if (n <= 0) return;
     const ShotDesc &A = shots[cb];  // geometry and coefficients of the chunk
@@ -609,7 +609,7 @@ __global__ void __launch_bounds__(TG / GPT * TX + 32)
            const __grid_constant__ CUtensorMap tm_cf, const ShotDesc *__restrict__ shots, const int4 *__restrict__ prog,
            int L, int shot_base, int nshot, int chunk, int *err)
 {
-    tile_body<TX, NST, MATH, GPT, 1>(tm_p1, tm_p0, tm_cf, shots, prog, L, shot_base, nshot, chunk, err);
+    tile_body<TX, NST, MATH, GPT, 1>(tm_p1, tm_p0, tm_cf, shots, prog, L, shot_base, nshot, chunk, err, blockIdx.y);
 }
 
 // the same step compiled for three blocks per SM, one group per thread, coefficients read from
@@ -620,7 +620,41 @@ __global__ void __launch_bounds__(TG * TX + 32, 3)
             const __grid_constant__ CUtensorMap tm_cf, const ShotDesc *__restrict__ shots, const int4 *__restrict__ prog,
             int L, int shot_base, int nshot, int chunk, int *err)
 {
-    tile_body<TX, NST, MATH, 1, 3>(tm_p1, tm_p0, tm_cf, shots, prog, L, shot_base, nshot, chunk, err);
+    tile_body<TX, NST, MATH, 1, 3>(tm_p1, tm_p0, tm_cf, shots, prog, L, shot_base, nshot, chunk, err, blockIdx.y);
+}
+
+// ------------------------------------------------------------ several groups in one launch
+// One shot group of a launch that advances several independent runs at once (the continuous
+// batching of the request loop): its own tensor maps (in global memory), shots, program and the
+// launch index at which its program started.  Groups are stacked along grid y; a block finds its
+// group by its row, and blocks outside the group's tiles or program return at once.
+struct __align__(128) TileGroup {
+    CUtensorMap p1, p0, cf;       // as the single-group kernel's parameters
+    const ShotDesc *shots;        // descriptors of the run's shots (shot_base .. shot_base + nshot - 1)
+    const int4 *prog;             // the group's current program
+    long long L0;                 // launch index of the program's item 0
+    int nprog;                    // items of the program
+    int shot_base, nshot, chunk;  // as the single-group kernel's parameters
+    int y0;                       // first grid row of the group (2 rows per chunk)
+    int ntx, zt;                  // column tiles (ntx: the receiver-sampling column) and z tiles
+};
+
+template <int TX, int NST, int MATH>
+__global__ void __launch_bounds__(TG * TX + 32, 3)
+    k_tile_groups(const TileGroup *__restrict__ groups, int ngroups, long long L, int *err)
+{
+    int g = 0;
+    while (g + 1 < ngroups && (int)blockIdx.y >= groups[g + 1].y0) ++g;
+    const TileGroup &T = groups[g];
+    const long long Lg = L - T.L0;
+    if (Lg < 0 || Lg >= T.nprog || (int)blockIdx.x > T.ntx || (int)blockIdx.z >= T.zt) return;
+    // the maps live in global memory, written before the launch: make them visible to the
+    // tensor-map proxy of this thread before its copies use them
+    asm volatile("fence.proxy.tensormap::generic.acquire.gpu [%0], 128;" ::"l"(&T.p1) : "memory");
+    asm volatile("fence.proxy.tensormap::generic.acquire.gpu [%0], 128;" ::"l"(&T.p0) : "memory");
+    asm volatile("fence.proxy.tensormap::generic.acquire.gpu [%0], 128;" ::"l"(&T.cf) : "memory");
+    tile_body<TX, NST, MATH, 1, 3>(T.p1, T.p0, T.cf, T.shots, T.prog, (int)Lg, T.shot_base, T.nshot, T.chunk, err,
+                                   (int)blockIdx.y - T.y0);
 }
 
 }  // namespace fwi

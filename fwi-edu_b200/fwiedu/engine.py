@@ -178,6 +178,46 @@ def propagation(vp, rho, shots, dx, dz, dt, nt, pml, fs, freq, filt, preconditio
     return pre, grad
 
 
+class Executor:
+    """Continuous batching (fwi_exec_*): runs of several contexts advanced by the same step
+    launches; a run added while others are in flight joins at the next launch."""
+
+    def __init__(self, device: int = 0):
+        self.L = lib()
+        self.h = C.c_void_p()
+        _check(self.L.fwi_exec_create(C.byref(self.h), device))
+
+    def add(self, ctx, problem, freq=0.0, filt=2, precondition=1):
+        _check(self.L.fwi_exec_add(self.h, ctx.h, int(problem), C.c_float(freq), int(filt), int(precondition)))
+
+    def step(self, launches=0):
+        """Issue up to `launches` step launches (0: until the batch is empty); runs left."""
+        a = C.c_int()
+        _check(self.L.fwi_exec_step(self.h, int(launches), C.byref(a)))
+        return a.value
+
+    def poll(self, ctx):
+        d, st = C.c_int(), C.c_int()
+        _check(self.L.fwi_exec_poll(self.h, ctx.h, C.byref(d), C.byref(st)))
+        return bool(d.value), st.value
+
+    def launches(self):
+        n = C.c_longlong()
+        _check(self.L.fwi_exec_launches(self.h, C.byref(n)))
+        return n.value
+
+    def close(self):
+        if self.h:
+            self.L.fwi_exec_destroy(self.h)
+            self.h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
 # fwi_allreduce_fn: int (*)(double *dev, size_t count, void *stream, void *user)
 ALLREDUCE_FN = C.CFUNCTYPE(C.c_int, C.c_void_p, C.c_size_t, C.c_void_p, C.c_void_p)
 

@@ -349,6 +349,29 @@ FWI_API int fwi_ctx_get_model(fwi_ctx *ctx, float *vp, float *rho);
  * stream is a cudaStream_t (NULL: the legacy default stream); the call only enqueues work. */
 FWI_API int fwi_smooth2d_noalloc(const float *d_in, float *d_out, int nx, int nz, int rz, int rx, void *stream);
 
+/* Continuous batching (no counterpart in the reference, whose runs go one at a time): an executor
+ * advances several independent runs -- each a context with its own model, grid size, record
+ * length and shots -- by the same step launches.  fwi_exec_add prepares a run of `problem`
+ * (0 modeling, 1 gradient, 2 line-search residual; freq, filter, precondition as for
+ * fwi_ctx_run) on a context whose model, shots and (problems 1, 2) observed data are set, and
+ * adds it to the batch: it joins at the next step launch, whatever the others' progress.
+ * fwi_exec_step issues up to `launches` step launches (<= 0: until the batch is empty), each
+ * advancing every run in the batch by one item of its own program, plus each run's work
+ * between its passes; *active = runs still in the batch.  A run whose last work is issued is
+ * handed back to its context (its stream ordered after that work): fwi_exec_poll then sets
+ * *done = 1 and *status, and the context's results are read as after fwi_ctx_run.  While a run
+ * is in the batch its context must not be used otherwise.  Results are bit-identical to
+ * fwi_ctx_run's batched path.  One thread may call fwi_exec_step while others call
+ * fwi_exec_add; the executor's arithmetic is FWI_MATH at creation and runs must match it.
+ * Snapshot output (verbose > 1) is not available here. */
+typedef struct fwi_exec fwi_exec;
+FWI_API int fwi_exec_create(fwi_exec **out, int device);
+FWI_API int fwi_exec_add(fwi_exec *ex, fwi_ctx *ctx, int problem, float freq, int filter, int precondition);
+FWI_API int fwi_exec_step(fwi_exec *ex, int launches, int *active);
+FWI_API int fwi_exec_poll(fwi_exec *ex, fwi_ctx *ctx, int *done, int *status);
+FWI_API int fwi_exec_launches(fwi_exec *ex, long long *launches);
+FWI_API int fwi_exec_destroy(fwi_exec *ex);
+
 /* Self-test of the failure path of the step kernel's waits (no counterpart in the reference): a
  * one-block kernel waits, with the step kernel's bounded wait and a limit of limit_ms (1..2000),
  * on an mbarrier phase that nothing completes; it gives up, sets the context's error word and

@@ -12,9 +12,10 @@ GOLDEN = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
 
 
 def names():
-    """The propagation cases (aux_*.npz hold fixtures of single functions)."""
+    """The propagation cases (aux_*.npz hold fixtures of single functions, demo_*.npz the expected
+    outputs of whole front-end runs)."""
     return sorted(os.path.splitext(os.path.basename(p))[0] for p in glob.glob(os.path.join(GOLDEN, "*.npz"))
-                  if not os.path.basename(p).startswith("aux_"))
+                  if not os.path.basename(p).startswith(("aux_", "demo_")))
 
 
 class Case:

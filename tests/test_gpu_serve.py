@@ -1,6 +1,7 @@
 """The serving loop (fwi_server_*): requests of mixed grid sizes admitted by device-memory
-footprint and run concurrently.  Every result must be the same alone and in the mix -- here
-bit for bit, since each request runs on its own deterministic context -- and the reference's
+footprint and batched continuously (the runs in flight share every step launch).  Every result
+must be the same alone and in the mix -- here bit for bit, since each run keeps its own
+deterministic state and the executor's arithmetic is the single run's -- and the reference's
 golden vectors still hold for the requests that have them.  Admission must keep the admitted
 footprint within the budget, and a request larger than the budget is refused at submission.
 """
