@@ -41,6 +41,7 @@
 #include "fwi_setup.h"
 #include "fwi_step.cuh"
 #include "fwi_tile.cuh"
+#include "fwi_tile2.cuh"
 #include "fwi_optim.cuh"
 #include "fwi_fft.cuh"
 
@@ -105,6 +106,7 @@ struct ShotRun {
 struct Program {
     std::vector<int4> items;
     int4 *d = nullptr;
+    int depth = 1;  // 2: items of the two-step kernel (fwi_tile2.cuh)
 };
 
 struct fwi_ctx {
@@ -138,6 +140,7 @@ struct fwi_ctx {
     std::map<std::string, cudaGraphExec_t> graphs;
     fwi_stats stats{};
     int math = 0;  // 0: bit-exact arithmetic, 1: contracted multiply-adds
+    int depth = 2;  // time steps per launch of the step kernel (1 or 2; FWI_DEPTH)
     bool use_graphs = true;  // capture the batched launch sequences as CUDA graphs
     bool pdl = true;         // consecutive steps as programmatic dependent launches
     bool tune = true;        // time the step kernel's launch shapes once per shape (autotune)
@@ -244,6 +247,7 @@ extern "C" int fwi_ctx_create(fwi_ctx **out, int device, size_t budget)
     c->device = device;
     c->budget = budget;
     if (const char *e = getenv("FWI_MATH")) c->math = atoi(e) ? 1 : 0;
+    if (const char *e = getenv("FWI_DEPTH")) c->depth = atoi(e) == 1 ? 1 : 2;
     if (const char *e = getenv("FWI_GRAPH")) c->use_graphs = e[0] != '0';  // 0: direct launches (profilers)
     if (const char *e = getenv("FWI_PDL")) c->pdl = e[0] != '0';
     if (const char *e = getenv("FWI_TUNE")) c->tune = e[0] != '0';            // 0: heuristic launch shapes
@@ -520,6 +524,21 @@ static int encode_group_maps(const ShotDesc &d0, int nshot, const float *coef, C
     return FWI_OK;
 }
 
+// the three maps of the two-step kernel: u(t) with a two-radius halo, u(t-1) and the
+// coefficients on the tile grown by one radius
+template <int TX>
+static int encode_group_maps2(const ShotDesc &d0, int nshot, const float *coef, CUtensorMap *ma, CUtensorMap *mb,
+                              CUtensorMap *cf)
+{
+    using Geo = Tile2Geom<TX>;
+    const long long pd[4] = {d0.ld, d0.Nx, d0.nfr, nshot}, cd[3] = {d0.ld, d0.Nx, 6};
+    const int ba[4] = {4 * Geo::AG, Geo::AX, 1, 1}, bb[4] = {4 * Geo::CG, Geo::CX, 1, 1}, bc[3] = {4 * Geo::CG, Geo::CX, 6};
+    TRY(encode_map(ma, d0.frames, 4, pd, ba));
+    TRY(encode_map(mb, d0.frames, 4, pd, bb));
+    TRY(encode_map(cf, coef, 3, cd, bc));
+    return FWI_OK;
+}
+
 // frame blocks of a group of runs, consecutive in one pool; a new pool or a new layout
 // invalidates the captured launches (their tensor maps hold the old one)
 static int assign_pool(fwi_ctx *c, int key, const std::vector<ShotRun *> &rs)
@@ -590,7 +609,7 @@ static int prepare_run(fwi_ctx *c, ShotRun *r, int shot, bool gradient)
         TRY(ralloc(c, r, &q, (size_t)ntr * 4)); d.recK = (float *)q;
         TRY(ralloc(c, r, &q, (size_t)ntr * 4)); d.rec_off = (int *)q;
         TRY(ralloc(c, r, &q, (size_t)s.ns * ntr * 4)); d.traces_t = (float *)q;
-        d.nfr = gradient ? nframes_gradient(d.K, d.S5) : 3;
+        d.nfr = gradient ? nframes_gradient(d.K, d.S5) : NROT;
         d.frames = nullptr;  // in the group's pool (assign_pool)
         d.H = d.Gacc = nullptr;
         d.adj_t = nullptr;
@@ -751,12 +770,66 @@ static std::vector<int4> program_adjoint(int nt, bool overlap)
     return prog;
 }
 
+// Programs of the two-step kernel (fwi_tile2.cuh): an item flagged K_DEPTH2 advances two
+// consecutive steps of its kind.  Forward: pairs (0, 1), (2, 3), ... and a last single step when
+// nt is odd.
+static std::vector<int4> program_forward2(int nt, int kind)
+{
+    std::vector<int4> p;
+    for (int it = 0; it < nt; it += 2) p.push_back(make_int4(it + 1 < nt ? kind | K_DEPTH2 : kind, it, K_NONE, 0));
+    return p;
+}
+
+// Adjoint pass of the two-step kernel: the overlapped schedule of program_adjoint with up to two
+// replay steps (consecutive, one segment) and up to two adjoint steps (it, it - 1) per launch.  A
+// replay step may run once the adjoint no longer needs the kept frames its segment overwrites;
+// an adjoint step once its imaging step's segment was replayed in an earlier launch.
+static std::vector<int4> program_adjoint2(int nt)
+{
+    const int d = fwi_ck_interval(nt), K = (nt - 1) / d;
+    auto top_of = [&](int k) { return k == K ? nt - 1 : k * d + d - 2; };
+    std::deque<int2> rq;
+    std::vector<int> need(K + 1, 0), done(K + 1, 0);
+    for (int k = K; k >= 0; --k) {
+        int cc = k * d, top = top_of(k);
+        for (int itt = cc; itt < top; ++itt) rq.push_back(make_int2(k, itt));
+        need[k] = std::max(0, top - cc);
+    }
+    std::vector<int4> prog;
+    int a = nt - 1;
+    while (!rq.empty() || a >= 0) {
+        int4 item = make_int4(K_NONE, 0, K_NONE, 0);
+        int nrep = 0, rep_k = -1, rep0 = 0;
+        while (nrep < 2 && !rq.empty()) {
+            const int k = rq.front().x, itt = rq.front().y;
+            if (nrep && (k != rep_k || itt != rep0 + 1)) break;
+            if (!((k + 2 > K) || (a <= (k + 2) * d))) break;
+            if (!nrep) rep0 = itt;
+            rep_k = k;
+            rq.pop_front();
+            ++nrep;
+        }
+        int nadj = 0, adj0 = a;
+        while (nadj < 2 && a >= 0 && (is_stored(a, nt, d) || done[a / d] >= need[a / d])) {
+            --a;
+            ++nadj;
+        }
+        if (nrep) item.x = nrep == 2 ? K_REP | K_DEPTH2 : K_REP, item.y = rep0;
+        if (nadj) item.z = nadj == 2 ? K_ADJ | K_DEPTH2 : K_ADJ, item.w = adj0;
+        if (rep_k >= 0) done[rep_k] += nrep;
+        prog.push_back(item);
+    }
+    return prog;
+}
+
 static int get_program(fwi_ctx *c, const std::string &key, const std::vector<int4> &items, Program **out)
 {
     auto it = c->progs.find(key);
     if (it == c->progs.end()) {
         Program p;
         p.items = items;
+        for (const int4 &w : items)
+            if ((w.x & K_DEPTH2) || (w.z & K_DEPTH2)) p.depth = 2;
         TRY(dmalloc(c, (void **)&p.d, items.size() * sizeof(int4)));
         CK(cudaMemcpy(p.d, items.data(), items.size() * sizeof(int4), cudaMemcpyHostToDevice));
         it = c->progs.emplace(key, std::move(p)).first;
@@ -871,9 +944,59 @@ struct TileCfg {
     int minb = 1;                              // 3: the three-blocks-per-SM variant (tx 16, gpt 1)
 };
 
+typedef void (*Tile2Fn)(const CUtensorMap, const CUtensorMap, const CUtensorMap, const ShotDesc *, const int4 *, int,
+                        int, int, int, int *);
+
+template <int NST, int MATH>
+static Tile2Fn tile2_fn()
+{
+    static bool ready = false;
+    Tile2Fn f = k_tile2<16, NST, MATH>;
+    if (!ready) {
+        cudaFuncSetAttribute((const void *)f, cudaFuncAttributeMaxDynamicSharedMemorySize, Tile2Geom<16>::smem(NST));
+        cudaFuncSetAttribute((const void *)f, cudaFuncAttributePreferredSharedMemoryCarveout,
+                             cudaSharedmemCarveoutMaxShared);
+        ready = true;
+    }
+    return f;
+}
+
+// launches of a two-step program: 16-column tiles, ring depth 2 or 3, the shape's chunk
+static int launch_tiles2(fwi_ctx *c, const Program *prog, int L0, int L1, int shot_base, int nshot, const ShotRun *r0,
+                         const TileCfg &cfg)
+{
+    const Plan *p = r0->plan;
+    const int zt = (p->G + TG - 1) / TG, tx = 16;
+    const int nst = cfg.nst >= 3 ? 3 : 2, chunk = cfg.chunk;
+    Tile2Fn fn = c->math ? (nst == 3 ? tile2_fn<3, 1>() : tile2_fn<2, 1>()) : (nst == 3 ? tile2_fn<3, 0>() : tile2_fn<2, 0>());
+    const int ntx = (p->Nx + tx - 1) / tx, nchunks = (nshot + chunk - 1) / chunk;
+    CUtensorMap ma, mb, mc;
+    TRY(encode_group_maps2<16>(r0->d, nshot, p->d_coef, &ma, &mb, &mc));
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    attr[0].val.programmaticStreamSerializationAllowed = 1;
+    cudaLaunchConfig_t lc = {};
+    lc.gridDim = dim3(ntx, 2 * nchunks, zt);
+    lc.blockDim = dim3(TG, tx + 32 / TG);
+    lc.dynamicSmemBytes = Tile2Geom<16>::smem(nst);
+    lc.stream = c->stream;
+    lc.attrs = attr;
+    lc.numAttrs = c->pdl ? 1 : 0;
+    for (int L = L0; L < L1; L++) {
+        const int4 &pw = prog->items[L];
+        if (pw.x == K_NONE && pw.z == K_NONE) continue;
+        CK(cudaLaunchKernelEx(&lc, fn, ma, mb, mc, (const ShotDesc *)c->d_desc, (const int4 *)prog->d, L, shot_base,
+                              nshot, chunk, c->d_err));
+        c->launches++;
+    }
+    CK(cudaGetLastError());
+    return FWI_OK;
+}
+
 static int launch_tiles(fwi_ctx *c, const Program *prog, int L0, int L1, int shot_base, int nshot, const ShotRun *r0,
                         const TileCfg &cfg)
 {
+    if (prog->depth == 2) return launch_tiles2(c, prog, L0, L1, shot_base, nshot, r0, cfg);
     const Plan *p = r0->plan;
     const int zt = (p->G + TG - 1) / TG;
     const int tx = cfg.tx, nst = cfg.nst, chunk = cfg.chunk, gpt = cfg.gpt, nl = TG / gpt;
@@ -912,26 +1035,26 @@ static int launch_tiles(fwi_ctx *c, const Program *prog, int L0, int L1, int sho
 
 // the measured best configuration per launch shape, shared by every context of the process
 struct TuneKey {
-    int Nx, G, nshot, math, batched;
+    int Nx, G, nshot, math, batched, depth;
     bool operator<(const TuneKey &o) const
     {
-        return std::tie(Nx, G, nshot, math, batched) < std::tie(o.Nx, o.G, o.nshot, o.math, o.batched);
+        return std::tie(Nx, G, nshot, math, batched, depth) < std::tie(o.Nx, o.G, o.nshot, o.math, o.batched, o.depth);
     }
 };
 static std::mutex g_tune_mu;
 static std::map<TuneKey, TileCfg> g_tune;
 
 // the heuristic shape, or the tuned one, with the environment's overrides applied last
-static TileCfg tile_config(fwi_ctx *c, const Plan *p, int nshot, bool batched)
+static TileCfg tile_config(fwi_ctx *c, const Plan *p, int nshot, bool batched, int depth = 1)
 {
     TileCfg cfg;
-    cfg.tx = batched ? 16 : 8;
-    cfg.nst = 4;
+    cfg.tx = batched || depth == 2 ? 16 : 8;
+    cfg.nst = depth == 2 ? 2 : 4;
     const int zt = (p->G + TG - 1) / TG;
     cfg.chunk = pick_chunk(((p->Nx + cfg.tx - 1) / cfg.tx) * zt, nshot, cfg.tx == 16 ? 2 : 4);
     {
         std::lock_guard<std::mutex> lk(g_tune_mu);
-        auto it = g_tune.find({p->Nx, p->G, nshot, c->math, batched ? 1 : 0});
+        auto it = g_tune.find({p->Nx, p->G, nshot, c->math, batched ? 1 : 0, depth});
         if (it != g_tune.end()) cfg = it->second;
     }
     if (const char *e = getenv("FWI_TX")) cfg.tx = atoi(e) == 8 ? 8 : 16;
@@ -953,25 +1076,40 @@ static TileCfg tile_config(fwi_ctx *c, const Plan *p, int nshot, bool batched)
 // scratch frames are zeroed again afterwards, which is the state a pass starts from; the
 // samples the probe wrote are overwritten by the pass.  Candidates: tile width 8/16, ring
 // depth 2..4, and chunks of at most 4/8/12/16/24 shots (split evenly).
-static int autotune(fwi_ctx *c, int shot_base, int nshot, const ShotRun *r0, bool batched)
+static int autotune(fwi_ctx *c, int shot_base, int nshot, const ShotRun *r0, bool batched, int depth = 1)
 {
     const Plan *p = r0->plan;
-    const TuneKey key{p->Nx, p->G, nshot, c->math, batched ? 1 : 0};
+    const TuneKey key{p->Nx, p->G, nshot, c->math, batched ? 1 : 0, depth};
     {
         std::lock_guard<std::mutex> lk(g_tune_mu);
         if (g_tune.count(key)) return FWI_OK;
     }
     const int steps = std::min(12, std::max(2, c->nt - 2));
     std::vector<int4> items;
-    for (int it = 1; it <= steps; it++) items.push_back(make_int4(K_FWD0, it, K_NONE, 0));
+    if (depth == 2)  // the same steps, two per launch
+        for (int it = 1; it + 1 <= steps; it += 2) items.push_back(make_int4(K_FWD0 | K_DEPTH2, it, K_NONE, 0));
+    else
+        for (int it = 1; it <= steps; it++) items.push_back(make_int4(K_FWD0, it, K_NONE, 0));
+    const int launches = (int)items.size();
     Program *prog;
-    TRY(get_program(c, "tune/" + std::to_string(steps), items, &prog));
+    TRY(get_program(c, (depth == 2 ? "tune2/" : "tune/") + std::to_string(steps), items, &prog));
     std::vector<TileCfg> cands;
     std::set<int> chunks;  // even splits of the shots into blocks of at most 4 .. 24
     for (int cap : {4, 8, 12, 16, 24}) {
         const int nch = (nshot + cap - 1) / cap;
         chunks.insert((nshot + nch - 1) / nch);
     }
+    if (depth == 2)  // the two-step kernel: 16-column tiles, ring depth 2 or 3
+        for (int nst : {2, 3})
+            for (int ch : chunks) {
+                if (nshot == 1 && nst != 2) continue;
+                TileCfg t;
+                t.tx = 16;
+                t.nst = nst;
+                t.chunk = ch;
+                cands.push_back(t);
+            }
+    else
     for (int gpt : {1, 2})
         for (int tx : {16, 8})
             for (int minb : {1, 3}) {
@@ -995,9 +1133,9 @@ static int autotune(fwi_ctx *c, int shot_base, int nshot, const ShotRun *r0, boo
     CK(cudaEventCreate(&e0));
     CK(cudaEventCreate(&e1));
     for (const TileCfg &t : cands) {
-        TRY(launch_tiles(c, prog, 0, std::min(3, steps), shot_base, nshot, r0, t));  // warm-up
+        TRY(launch_tiles(c, prog, 0, std::min(3, launches), shot_base, nshot, r0, t));  // warm-up
         CK(cudaEventRecord(e0, c->stream));
-        TRY(launch_tiles(c, prog, 0, steps, shot_base, nshot, r0, t));
+        TRY(launch_tiles(c, prog, 0, launches, shot_base, nshot, r0, t));
         CK(cudaEventRecord(e1, c->stream));
         CK(cudaEventSynchronize(e1));
         float ms = 0.f;
@@ -1012,7 +1150,7 @@ static int autotune(fwi_ctx *c, int shot_base, int nshot, const ShotRun *r0, boo
     c->launches = l0;  // probe launches are not part of the run
     for (int i = 0; i < nshot; i++) {
         const ShotRun *r = c->runs.size() == 1 ? c->runs[0].get() : c->runs[shot_base + i].get();
-        CK(cudaMemsetAsync(frame_ptr(r->d, F_FWD), 0, 3 * (size_t)r->d.frame * 4, c->stream));
+        CK(cudaMemsetAsync(frame_ptr(r->d, F_FWD), 0, NROT * (size_t)r->d.frame * 4, c->stream));
     }
     TRY(check_kernel_error(c));
     std::lock_guard<std::mutex> lk(g_tune_mu);
@@ -1039,7 +1177,7 @@ static int launch_steps(fwi_ctx *c, const Program *prog, int shot_base, int nsho
         CK(cudaGetLastError());
         return FWI_OK;
     }
-    const TileCfg cfg = tile_config(c, p, nshot, batched);
+    const TileCfg cfg = tile_config(c, p, nshot, batched, prog->depth);
     return launch_tiles(c, prog, 0, n, shot_base, nshot, r0, cfg);
 }
 
@@ -1379,15 +1517,22 @@ static int conv_tables(fwi_ctx *c, const std::string &key, int n, const std::fun
     if (M > FFT_CONV_MAX)
         return fail(FWI_ERR_UNSUPPORTED, "FFT convolution of length %d needs %d points (at most %d)", n, M,
                     FFT_CONV_MAX);
+    const bool f64 = conv_in_f64(M);
     const float *G, *tw;
-    TRY(device_operator(c, "spec/" + key, (size_t)2 * M, [&](float *out) {
+    // FP64 tables take 4M / 2M floats' room (double2), FP32 ones 2M / M
+    TRY(device_operator(c, (f64 ? "spec64/" : "spec/") + key, (size_t)(f64 ? 4 : 2) * M, [&](float *out) {
         std::vector<double> h(n);
         kernel(h.data());
-        fwi_conv_spectrum(h.data(), n, M, out);
+        if (f64) fwi_conv_spectrum_f64(h.data(), n, M, reinterpret_cast<double *>(out));
+        else fwi_conv_spectrum(h.data(), n, M, out);
     }, &G));
-    TRY(device_operator(c, "tw/" + std::to_string(M), (size_t)M, [&](float *out) { fwi_fft_twiddles(M, out); }, &tw));
-    d->G = (const float2 *)G;
-    d->tw = (const float2 *)tw;
+    TRY(device_operator(c, (f64 ? "tw64/" : "tw/") + std::to_string(M), (size_t)(f64 ? 2 : 1) * M, [&](float *out) {
+        if (f64) fwi_fft_twiddles_f64(M, reinterpret_cast<double *>(out));
+        else fwi_fft_twiddles(M, out);
+    }, &tw));
+    d->G = G;
+    d->tw = tw;
+    d->dbl = f64 ? 1 : 0;
     d->N = n;
     return FWI_OK;
 }
@@ -1624,7 +1769,7 @@ static int stack_and_precondition(fwi_ctx *c, const std::vector<ShotRun *> &rs, 
 static int zero_initial(fwi_ctx *c, ShotRun *r, bool gradient)
 {
     const size_t fb = (size_t)r->d.frame * 4;
-    CK(cudaMemsetAsync(frame_ptr(r->d, F_FWD), 0, 3 * fb, c->stream));
+    CK(cudaMemsetAsync(frame_ptr(r->d, F_FWD), 0, NROT * fb, c->stream));
     if (gradient) {
         CK(cudaMemsetAsync(frame_ptr(r->d, F_CK), 0, 2 * fb, c->stream));  // u(-1), u(0)
         CK(cudaMemsetAsync(r->d.H, 0, (size_t)r->d.frame * 8, c->stream));
@@ -1675,7 +1820,8 @@ static int run_program(fwi_ctx *c, const std::string &key, const Program *prog, 
     }
     if (!batched) return launch_steps(c, prog, shot_base, nshot, r0, false);
     if (!c->use_graphs) return launch_steps(c, prog, shot_base, nshot, r0, true);
-    auto it = c->graphs.find(key);
+    const std::string gk = key + "#" + std::to_string(prog->depth);  // graphs of one- and two-step programs differ
+    auto it = c->graphs.find(gk);
     if (it == c->graphs.end()) {
         cudaGraph_t g;
         CK(cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal));
@@ -1689,7 +1835,7 @@ static int run_program(fwi_ctx *c, const std::string &key, const Program *prog, 
         cudaGraphDestroy(g);
         if (e != cudaSuccess) return fail(FWI_ERR_CUDA, "graph instantiate: %s", cudaGetErrorString(e));
         c->launches = before;
-        it = c->graphs.emplace(key, ge).first;
+        it = c->graphs.emplace(gk, ge).first;
     }
     CK(cudaGraphLaunch(it->second, c->stream));
     c->stats.graph_launches++;
@@ -1708,7 +1854,7 @@ static int timed_program(fwi_ctx *c, int kind, const std::string &key, const Pro
     const bool tile_kernel = !(ke && strcmp(ke, "step") == 0);
     if (c->tune && tile_kernel && !getenv("FWI_TX") && !getenv("FWI_NST") && !getenv("FWI_CHUNK") && !getenv("FWI_GPT") &&
         !getenv("FWI_OCC"))
-        TRY(autotune(c, shot_base, nshot, r0, batched));
+        TRY(autotune(c, shot_base, nshot, r0, batched, prog->depth));
     fwi_ctx::PassTimer &t = c->pass[kind];
     if (t.used == t.ev.size()) {
         cudaEvent_t a, b;
@@ -1725,11 +1871,33 @@ static int timed_program(fwi_ctx *c, int kind, const std::string &key, const Pro
     return FWI_OK;
 }
 
+// time steps per launch of the step kernel for this run: the context's (two unless FWI_DEPTH=1),
+// one for runs that write snapshots and for the cp.async comparison kernel
+static int run_depth(const fwi_ctx *c)
+{
+    const char *ke = getenv("FWI_KERNEL");
+    if (c->dump.verbose > 1 || (ke && strcmp(ke, "step") == 0)) return 1;
+    return c->depth;
+}
+
+static int forward_program(fwi_ctx *c, int kind, Program **out)
+{
+    const bool two = run_depth(c) == 2;
+    const std::string key = std::string(kind == K_FWD1 ? "fwd1" : "fwd0") + (two ? "x2" : "");
+    return get_program(c, key, two ? program_forward2(c->nt, kind) : program_forward(c->nt, kind), out);
+}
+
+static int adjoint_program(fwi_ctx *c, bool batched, Program **out)
+{
+    if (run_depth(c) == 2) return get_program(c, "adj/x2", program_adjoint2(c->nt), out);
+    return get_program(c, batched ? "adj/overlap" : "adj/plain", program_adjoint(c->nt, batched), out);
+}
+
 static int run_forward_group(fwi_ctx *c, std::vector<ShotRun *> &rs, int problem, float freq, int filter, bool batched,
                              const std::string &gkey, int shot_base)
 {
     Program *prog;
-    TRY(get_program(c, "fwd0", program_forward(c->nt, K_FWD0), &prog));
+    TRY(forward_program(c, K_FWD0, &prog));
     for (ShotRun *r : rs) TRY(zero_initial(c, r, false));
     TRY(timed_program(c, 0, "fwd0/" + gkey, prog, shot_base, (int)rs.size(), rs[0], batched));
     if (problem == 2) {
@@ -1746,7 +1914,7 @@ static int grad_forward(fwi_ctx *c, std::vector<ShotRun *> &rs, int precondition
                         const std::string &gkey, int shot_base)
 {
     Program *pf;
-    TRY(get_program(c, "fwd1", program_forward(c->nt, K_FWD1), &pf));
+    TRY(forward_program(c, K_FWD1, &pf));
     for (ShotRun *r : rs) TRY(zero_initial(c, r, true));
     TRY(timed_program(c, 0, "fwd1/" + gkey, pf, shot_base, (int)rs.size(), rs[0], batched));
     if (precondition == 1) TRY(finalize(c, rs, 0));
@@ -1757,7 +1925,7 @@ static int grad_forward(fwi_ctx *c, std::vector<ShotRun *> &rs, int precondition
 static int grad_adjoint(fwi_ctx *c, std::vector<ShotRun *> &rs, bool batched, const std::string &gkey, int shot_base)
 {
     Program *pa;
-    TRY(get_program(c, batched ? "adj/overlap" : "adj/plain", program_adjoint(c->nt, batched), &pa));
+    TRY(adjoint_program(c, batched, &pa));
     TRY(adj_init(c, rs, shot_base));
     TRY(timed_program(c, 1, std::string(batched ? "adjo/" : "adjp/") + gkey, pa, shot_base, (int)rs.size(), rs[0],
                       batched));
@@ -2072,7 +2240,7 @@ extern "C" size_t fwi_estimate_bytes(const fwi_shot *shots, int nshot, int nz, i
         b += 3 * rec * 4;                                                // observed, predicted, line-search gathers
         b += (size_t)nt * 12 + (Nx + 1) * 4 + (size_t)s.ntr * 16 + rec * 4;  // source terms, receivers, samples
         b += ((size_t)s.ns + 1 + s.ntr + 1) * 4;                         // taper coefficients
-        b += (grad ? (size_t)nframes_gradient(K, S5) : 3) * frame * 4;   // frame block in the pool
+        b += (grad ? (size_t)nframes_gradient(K, S5) : NROT) * frame * 4;  // frame block in the pool
         if (grad) b += 2 * frame * 8 + (size_t)nt * s.ntr * 4 + 2 * (size_t)nz * nxx * 4;
         max_ns = std::max(max_ns, (size_t)s.ns);
         max_ntr = std::max(max_ntr, (size_t)s.ntr);
@@ -2093,7 +2261,7 @@ extern "C" size_t fwi_estimate_bytes(const fwi_shot *shots, int nshot, int nz, i
 extern "C" int fwi_adjoint_program(int nt, int overlap, int *items, int cap)
 {
     if (nt <= 0) return 0;
-    std::vector<int4> p = program_adjoint(nt, overlap != 0);
+    std::vector<int4> p = overlap == 2 ? program_adjoint2(nt) : program_adjoint(nt, overlap != 0);
     if (items)
         for (int i = 0; i < (int)p.size() && i < cap; i++) {
             items[4 * i] = p[i].x;

@@ -236,11 +236,11 @@ extern "C" int fwi_exec_add(fwi_exec *ex, fwi_ctx *c, int problem, float freq, i
     return FWI_OK;
 }
 
-// the launch table: every group of every run in the batch, stacked along grid y
+// the launch table: every group of every run in the batch, one flat block range each
 static int exec_table(fwi_exec *ex)
 {
     std::vector<TileGroup> t;
-    int y = 0, gx = 1, gz = 1;
+    long long nb = 0;
     for (ExecRun *er : ex->runs)
         for (auto &g : er->groups) {
             TileGroup T;
@@ -255,14 +255,15 @@ static int exec_table(fwi_exec *ex)
             T.shot_base = g.shot_base;
             T.nshot = g.nshot;
             T.chunk = g.chunk;
-            T.y0 = y;
             T.ntx = g.ntx;
             T.zt = g.zt;
-            y += 2 * ((g.nshot + g.chunk - 1) / g.chunk);
-            gx = std::max(gx, g.ntx + 1);
-            gz = std::max(gz, g.zt);
+            T.halves = er->phase == 1 ? 2 : 1;  // the adjoint program pairs replay and adjoint items
+            T.b0 = (int)nb;
+            T.nblk = (g.ntx + 1) * g.zt * T.halves * ((g.nshot + g.chunk - 1) / g.chunk);
+            nb += T.nblk;
             t.push_back(T);
         }
+    if (nb > 0x7fffffff) return fail(FWI_ERR_UNSUPPORTED, "too many blocks in one launch of the batch");
     if ((int)t.size() > ex->groups_cap) {
         if (ex->d_groups) {
             CK(cudaStreamSynchronize(ex->stream));
@@ -274,7 +275,7 @@ static int exec_table(fwi_exec *ex)
     if (!t.empty())  // pageable source: staged before the call returns, ordered after the last launch
         CK(cudaMemcpyAsync(ex->d_groups, t.data(), t.size() * sizeof(TileGroup), cudaMemcpyHostToDevice, ex->stream));
     ex->ngroups = (int)t.size();
-    ex->grid = dim3(gx, std::max(y, 1), gz);
+    ex->grid = dim3((unsigned)std::max<long long>(nb, 1), 1, 1);
     ex->dirty = false;
     return FWI_OK;
 }

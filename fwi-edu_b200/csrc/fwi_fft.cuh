@@ -15,9 +15,9 @@
 // One block holds P such pairs in shared memory (P * M complex floats): the sequences are
 // loaded bit-reversed, transformed by radix-2 decimation in time (natural order out),
 // multiplied by G, transformed back by decimation in frequency with conjugate twiddles
-// (bit-reversed order out) and written from the bit-reversed positions.  FP32 throughout;
-// the reference's own result carries its FFT library's FP32 rounding, so agreement is to
-// FP32 tolerance, not bitwise.
+// (bit-reversed order out) and written from the bit-reversed positions.  FP64 transforms where
+// a block holds them (M <= 8192), FP32 above; agreement with the reference is to floating-point
+// tolerance, not bitwise (its result carries its own FFT's rounding).
 #pragma once
 #include <cuda_runtime.h>
 
@@ -35,23 +35,42 @@ struct ConvDesc {
     int nseq;                   // sequences
     int M, logM;                // FFT size, a power of two >= 2N - 1
     int P;                      // sequence pairs per block
-    const float2 *G;            // FFT_M of the wrapped kernel, / M
-    const float2 *tw;           // exp(-2 pi i k / M), k < M / 2
+    int dbl;                    // 1: transforms in FP64 (G and tw double2), 0: FP32 (float2)
+    const void *G;              // FFT_M of the wrapped kernel, / M
+    const void *tw;             // exp(-2 pi i k / M), k < M / 2
 };
 
-__device__ __forceinline__ float2 cmulf(float2 a, float2 b)
+template <class R> struct Cplx;
+template <> struct Cplx<float> {
+    typedef float2 T;
+    static __device__ __forceinline__ T make(float a, float b) { return make_float2(a, b); }
+};
+template <> struct Cplx<double> {
+    typedef double2 T;
+    static __device__ __forceinline__ T make(double a, double b) { return make_double2(a, b); }
+};
+
+template <class T>
+__device__ __forceinline__ T cmulc(T a, T b)
 {
-    return make_float2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
+    T r;
+    r.x = a.x * b.x - a.y * b.y;
+    r.y = a.x * b.y + a.y * b.x;
+    return r;
 }
 
-// grid: ceil(nseq / (2 P)) blocks; dynamic shared memory P * M float2
+// grid: ceil(nseq / (2 P)) blocks; dynamic shared memory P * M complex values of type R
+template <class R>
 static __global__ void __launch_bounds__(512) k_fft_conv(const ConvDesc d)
 {
-    extern __shared__ float2 fbuf[];
+    typedef typename Cplx<R>::T C;
+    extern __shared__ __align__(16) unsigned char fsm[];
+    C *fbuf = reinterpret_cast<C *>(fsm);
+    const C *G = static_cast<const C *>(d.G), *tw = static_cast<const C *>(d.tw);
     const int M = d.M, P = d.P, half_M = M >> 1;
     const int s0 = blockIdx.x * 2 * P;  // first sequence of the block
     const int tid = threadIdx.x, nth = blockDim.x;
-    for (int i = tid; i < P * M; i += nth) fbuf[i] = make_float2(0.f, 0.f);
+    for (int i = tid; i < P * M; i += nth) fbuf[i] = Cplx<R>::make(0, 0);
     __syncthreads();
     // load: pair q holds sequences s0 + 2q (real part) and s0 + 2q + 1 (imaginary part); the
     // sequence index runs fastest so that neighbouring threads read neighbouring addresses when
@@ -61,8 +80,8 @@ static __global__ void __launch_bounds__(512) k_fft_conv(const ConvDesc d)
         const int j = t / nsb, sl = t % nsb;
         const float v = d.in[(long long)(s0 + sl) * d.in_ss + (long long)j * d.in_es];
         const unsigned pos = __brev((unsigned)(j * d.stuff)) >> (32 - d.logM);
-        float *c = reinterpret_cast<float *>(&fbuf[(sl >> 1) * M + pos]);
-        c[sl & 1] = v;
+        R *c = reinterpret_cast<R *>(&fbuf[(sl >> 1) * M + pos]);
+        c[sl & 1] = (R)v;
     }
     __syncthreads();
     // forward: decimation in time, bit-reversed in, natural order out
@@ -71,14 +90,14 @@ static __global__ void __launch_bounds__(512) k_fft_conv(const ConvDesc d)
         for (int b = tid; b < P * half_M; b += nth) {
             const int q = b / half_M, bb = b - q * half_M;
             const int p = bb & (half - 1), i = ((bb >> (lg - 1)) << lg) + p, j = i + half;
-            float2 *f = fbuf + q * M;
-            const float2 t = cmulf(__ldg(d.tw + p * tstep), f[j]), a = f[i];
-            f[i] = make_float2(a.x + t.x, a.y + t.y);
-            f[j] = make_float2(a.x - t.x, a.y - t.y);
+            C *f = fbuf + q * M;
+            const C t = cmulc(tw[p * tstep], f[j]), a = f[i];
+            f[i] = Cplx<R>::make(a.x + t.x, a.y + t.y);
+            f[j] = Cplx<R>::make(a.x - t.x, a.y - t.y);
         }
         __syncthreads();
     }
-    for (int i = tid; i < P * M; i += nth) fbuf[i] = cmulf(fbuf[i], __ldg(d.G + (i & (M - 1))));
+    for (int i = tid; i < P * M; i += nth) fbuf[i] = cmulc(fbuf[i], G[i & (M - 1)]);
     __syncthreads();
     // inverse: decimation in frequency with conjugate twiddles, natural in, bit-reversed out
     for (int len = M, lg = d.logM; len >= 2; len >>= 1, --lg) {
@@ -86,10 +105,10 @@ static __global__ void __launch_bounds__(512) k_fft_conv(const ConvDesc d)
         for (int b = tid; b < P * half_M; b += nth) {
             const int q = b / half_M, bb = b - q * half_M;
             const int p = bb & (half - 1), i = ((bb >> (lg - 1)) << lg) + p, j = i + half;
-            float2 *f = fbuf + q * M;
-            const float2 w = __ldg(d.tw + p * tstep), a = f[i], c = f[j];
-            f[i] = make_float2(a.x + c.x, a.y + c.y);
-            f[j] = cmulf(make_float2(a.x - c.x, a.y - c.y), make_float2(w.x, -w.y));
+            C *f = fbuf + q * M;
+            const C w = tw[p * tstep], a = f[i], c = f[j];
+            f[i] = Cplx<R>::make(a.x + c.x, a.y + c.y);
+            f[j] = cmulc(Cplx<R>::make(a.x - c.x, a.y - c.y), Cplx<R>::make(w.x, -w.y));
         }
         __syncthreads();
     }
@@ -98,33 +117,42 @@ static __global__ void __launch_bounds__(512) k_fft_conv(const ConvDesc d)
         float v = 0.f;
         if (i < d.N) {
             const unsigned pos = __brev((unsigned)i) >> (32 - d.logM);
-            const float *c = reinterpret_cast<const float *>(&fbuf[(sl >> 1) * M + pos]);
-            v = c[sl & 1];
+            const R *c = reinterpret_cast<const R *>(&fbuf[(sl >> 1) * M + pos]);
+            v = (float)c[sl & 1];
         }
         d.out[(long long)(s0 + sl) * d.out_ss + (long long)i * d.out_es] = v;
     }
 }
 
-constexpr int FFT_CONV_MAX = 16384;  // largest M one block holds (128 KB of shared memory)
+constexpr int FFT_CONV_MAX = 16384;      // largest M one block holds in FP32 (128 KB of shared memory)
+constexpr int FFT_CONV_MAX_F64 = 8192;   // largest M one block holds in FP64 (128 KB)
+
+// The transforms run in FP64 where the block holds them (M <= 8192): the filtered residual can
+// be much smaller than the residual (a low-pass far below the source's band), and an FP32
+// transform's rounding, relative to the input, then shows in the output.
+static inline bool conv_in_f64(int M) { return M <= FFT_CONV_MAX_F64; }
 
 // fills M, logM and P of d (M from d.N, as fwi_conv_size) and launches; cudaErrorInvalidValue when
-// M > FFT_CONV_MAX or the sizes do not fit
+// M > FFT_CONV_MAX, the sizes do not fit, or d.dbl does not match conv_in_f64(M)
 static inline cudaError_t launch_fft_conv(ConvDesc d, cudaStream_t st)
 {
     int M = 2, lg = 1;  // the size fwi_conv_size gives, for which G and tw were built
     while (M < 2 * d.N - 1) M <<= 1, ++lg;
-    if (M > FFT_CONV_MAX || d.N < 1 || d.nseq < 1 || d.n_in < 1 || (d.n_in - 1) * d.stuff >= d.N)
+    if (M > FFT_CONV_MAX || d.N < 1 || d.nseq < 1 || d.n_in < 1 || (d.n_in - 1) * d.stuff >= d.N ||
+        (d.dbl != 0) != conv_in_f64(M))
         return cudaErrorInvalidValue;
     d.M = M;
     d.logM = lg;
-    d.P = M >= 8192 ? 1 : 8192 / M;  // up to 64 KB of pairs per block below the largest sizes
+    const size_t csize = d.dbl ? 16 : 8;
+    d.P = M >= 8192 ? 1 : 8192 / M;  // up to 64 KB (FP32) / 128 KB (FP64) of pairs per block
     d.P = d.P < (d.nseq + 1) / 2 ? d.P : (d.nseq + 1) / 2;
-    const size_t smem = (size_t)d.P * M * sizeof(float2);
-    cudaError_t e = cudaFuncSetAttribute((const void *)k_fft_conv, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                         (int)smem);
+    const size_t smem = (size_t)d.P * M * csize;
+    const void *fn = d.dbl ? (const void *)k_fft_conv<double> : (const void *)k_fft_conv<float>;
+    cudaError_t e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return e;
     const int blocks = (d.nseq + 2 * d.P - 1) / (2 * d.P);
-    k_fft_conv<<<blocks, 512, smem, st>>>(d);
+    if (d.dbl) k_fft_conv<double><<<blocks, 512, smem, st>>>(d);
+    else k_fft_conv<float><<<blocks, 512, smem, st>>>(d);
     return cudaGetLastError();
 }
 

@@ -41,7 +41,7 @@ struct ShotDesc {
     const float *adj_t;    // [nt][ntr] adjoint source
     // wavefield storage: one block of nfr frames of Nx*ld floats per shot (the blocks of a
     // shot group are consecutive in one pool, so one tensor map covers the group), laid out as
-    // F_FWD (3 forward frames), F_ADJ (3 adjoint), F_REP (3 replay), F_CK (2(K+1) checkpoint
+    // F_FWD (NROT forward frames), F_ADJ (NROT adjoint), F_REP (NROT replay), F_CK (2(K+1) checkpoint
     // slots: slot 0 = u(-1), 2k+1 = u(kd), 2k = u(kd-1)), then 2*S5 replayed frames kept for
     // imaging (t % 5 == 0), double-buffered by segment.  A forward-only run has nfr = 3.
     float *frames;
@@ -65,7 +65,11 @@ __host__ __device__ inline int stored_slot(const ShotDesc &S, int t)
     if ((t + 1) % S.d == 0 && t + 1 < S.nt) return 2 * ((t + 1) / S.d);
     return -1;
 }
-constexpr int F_FWD = 0, F_ADJ = 3, F_REP = 6, F_CK = 9;
+// Fields that are not kept rotate through NROT frames by time index.  Four, not three: a launch
+// that advances two steps (temporal blocking) reads u(t) and u(t-1) and writes u(t+1) and u(t+2),
+// and its blocks read halos of u(t-1) while others already write u(t+2): four distinct frames.
+constexpr int NROT = 4;
+constexpr int F_FWD = 0, F_ADJ = NROT, F_REP = 2 * NROT, F_CK = 3 * NROT;
 __host__ __device__ inline int nframes_gradient(int K, int S5) { return F_CK + 2 * (K + 1) + 2 * S5; }
 __host__ __device__ inline float *frame_ptr(const ShotDesc &S, int i) { return S.frames + (long long)i * S.frame; }
 
@@ -76,7 +80,7 @@ __host__ __device__ inline int fwd_idx(const ShotDesc &S, int t, bool keep)
         int s = stored_slot(S, t);
         if (s >= 0) return F_CK + s;
     }
-    return F_FWD + (t + 3) % 3;
+    return F_FWD + (t + NROT) % NROT;
 }
 // replayed frame of segment k (checkpoint c = k*d), t > c, t % 5 == 0
 __host__ __device__ inline int seg_idx(const ShotDesc &S, int t)
@@ -91,10 +95,10 @@ __host__ __device__ inline int rep_idx(const ShotDesc &S, int t)
     int s = stored_slot(S, t);
     if (s >= 0) return F_CK + s;
     if (t % MST == 0) return seg_idx(S, t);
-    return F_REP + t % 3;
+    return F_REP + t % NROT;
 }
 // adjoint field A(t): p1 of adjoint step t (with the injection of step t applied)
-__host__ __device__ inline int adj_idx(const ShotDesc &, int t) { return F_ADJ + (t + 3) % 3; }
+__host__ __device__ inline int adj_idx(const ShotDesc &, int t) { return F_ADJ + (t + NROT) % NROT; }
 // forward field used by the imaging condition at adjoint step it (it % 5 == 0)
 __host__ __device__ inline int img_idx(const ShotDesc &S, int it)
 {

@@ -120,9 +120,14 @@ void build_spectrum(float *out, const int *ip, const float *fp)
     std::vector<double> h(N);
     if (kind == 2) fwi_interp_kernel(n, r, h.data());
     else fwi_filter_kernel(kind, n, fp[0], fp[1], fp[2], h.data());
-    fwi_conv_spectrum(h.data(), N, M, out);
+    if (conv_in_f64(M)) fwi_conv_spectrum_f64(h.data(), N, M, reinterpret_cast<double *>(out));
+    else fwi_conv_spectrum(h.data(), N, M, out);
 }
-void build_twiddles(float *out, const int *ip, const float *) { fwi_fft_twiddles(ip[0], out); }
+void build_twiddles(float *out, const int *ip, const float *)
+{
+    if (conv_in_f64(ip[0])) fwi_fft_twiddles_f64(ip[0], reinterpret_cast<double *>(out));
+    else fwi_fft_twiddles(ip[0], out);
+}
 
 // the tables of a convolution of length N into d; false (with a message) when N is too long
 bool conv_tables(const Kernel1d &k, int N, ConvDesc *d)
@@ -132,16 +137,18 @@ bool conv_tables(const Kernel1d &k, int N, ConvDesc *d)
         fprintf(stderr, "<error>: FFT convolution of length %d needs %d points (at most %d)\n", N, M, FFT_CONV_MAX);
         return false;
     }
+    const bool f64 = conv_in_f64(M);
     const int ip[4] = {k.kind, k.n, k.r, N};
     const float fp[3] = {k.fpass, k.fcut, k.dt};
     const float *G = op_matrix("s" + std::to_string(k.kind) + "/" + std::to_string(k.n) + "/" + std::to_string(k.r) +
                                    "/" + fbits(k.fpass) + "/" + fbits(k.fcut) + "/" + fbits(k.dt),
-                               (size_t)2 * M, build_spectrum, ip, fp);
+                               (size_t)(f64 ? 4 : 2) * M, build_spectrum, ip, fp);
     const int ipt[1] = {M};
-    const float *tw = op_matrix("tw/" + std::to_string(M), (size_t)M, build_twiddles, ipt, nullptr);
+    const float *tw = op_matrix("tw/" + std::to_string(M), (size_t)(f64 ? 2 : 1) * M, build_twiddles, ipt, nullptr);
     if (!G || !tw) return false;
-    d->G = (const float2 *)G;
-    d->tw = (const float2 *)tw;
+    d->G = G;
+    d->tw = tw;
+    d->dbl = f64 ? 1 : 0;
     d->N = N;
     return true;
 }

@@ -391,6 +391,29 @@ void fwi_conv_spectrum(const double *h, int n, int M, float *G)
     free(im);
 }
 
+void fwi_conv_spectrum_f64(const double *h, int n, int M, double *G)
+{
+    double *re = (double *)calloc((size_t)M, sizeof(double)), *im = (double *)calloc((size_t)M, sizeof(double));
+    for (int m = 0; m < n; m++) re[m] = h[m];
+    for (int m = 1; m < n; m++) re[M - m] = h[n - m];
+    fft_pow2(re, im, M, -1);
+    for (int k = 0; k < M; k++) {
+        G[2 * k] = re[k] / M;
+        G[2 * k + 1] = im[k] / M;
+    }
+    free(re);
+    free(im);
+}
+
+void fwi_fft_twiddles_f64(int M, double *tw)
+{
+    for (int k = 0; k < M / 2; k++) {
+        const double a = 2.0 * 3.141592653589793 * k / M;
+        tw[2 * k] = cos(a);
+        tw[2 * k + 1] = -sin(a);
+    }
+}
+
 void fwi_fft_twiddles(int M, float *tw)
 {
     for (int k = 0; k < M / 2; k++) {

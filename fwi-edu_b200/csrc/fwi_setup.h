@@ -66,6 +66,9 @@ void fwi_interp_kernel(int ns, int r, double *g);
 int fwi_conv_size(int n);
 void fwi_conv_spectrum(const double *h, int n, int M, float *G);
 void fwi_fft_twiddles(int M, float *tw);
+/* the same two tables in FP64 (for transforms that run in FP64) */
+void fwi_conv_spectrum_f64(const double *h, int n, int M, double *G);
+void fwi_fft_twiddles_f64(int M, double *tw);
 
 /* lowpass2d (filter 0, common.c:1042-1162) / bandpass2d (filter 1, :1164-1284) window over the
  * full Nx x Nz wavenumber plane of the padded field, W[ix * Nz + iz], from the reference's float

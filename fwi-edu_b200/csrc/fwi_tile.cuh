@@ -272,7 +272,7 @@ struct TileGeom {
 template <int TX, int NST, int MATH, int GPT, int MINB>
 __device__ __forceinline__ void tile_body(const CUtensorMap &tm_p1, const CUtensorMap &tm_p0, const CUtensorMap &tm_cf,
                                           const ShotDesc *__restrict__ shots, const int4 *__restrict__ prog, int L,
-                                          int shot_base, int nshot, int chunk, int *err, int by)
+                                          int shot_base, int nshot, int chunk, int *err, int bx, int by, int bz)
 {
     using Geo = TileGeom<TX>;
     constexpr int NL = TG / GPT;  // consumer lanes per column
@@ -304,8 +304,8 @@ __device__ __forceinline__ void tile_body(const CUtensorMap &tm_p1, const CUtens
     const int warp = tid >> 5, lane = tid & 31;
 
     // ---- the receiver-sampling block: p1 is read-only during this launch
-    if ((int)blockIdx.x >= ntx) {
-        if (!fwd || it % A.sr != 0 || (int)blockIdx.x > ntx || blockIdx.z != 0) return;
+    if (bx >= ntx) {
+        if (!fwd || it % A.sr != 0 || bx > ntx || bz != 0) return;
         grid_dep_wait();
         for (int s = 0; s < n; ++s) {
             const ShotDesc &D = shots[cb + s];
@@ -316,7 +316,7 @@ __device__ __forceinline__ void tile_body(const CUtensorMap &tm_p1, const CUtens
         return;
     }
 
-    const int X0 = blockIdx.x * TX, G0 = blockIdx.z * TG;
+    const int X0 = bx * TX, G0 = bz * TG;
     unsigned char *st_base = smem + Geo::ST_OFF;
     const bool producer = warp == NW && lane == 0;
     int issued = 0;  // shots whose copies the producer has issued
@@ -360,7 +360,7 @@ __device__ __forceinline__ void tile_body(const CUtensorMap &tm_p1, const CUtens
         s_rz1[tid] = D.rz1;
         // does this tile need the rare parts of the epilogue for this shot (its source, its
         // receiver rows for the adjoint injection)?
-        const int X0t = blockIdx.x * TX, Z0t = 4 * blockIdx.z * TG;
+        const int X0t = bx * TX, Z0t = 4 * bz * TG;
         const bool src_t = (fwd || kind == K_REP) && D.isx >= X0t && D.isx < X0t + TX && D.isz >= Z0t &&
                            D.isz < Z0t + 4 * TG;
         const bool inj_t = kind == K_ADJ && it >= 1 && Z0t + 4 * TG > D.rz0 && Z0t <= D.rz1;
@@ -609,7 +609,8 @@ __global__ void __launch_bounds__(TG / GPT * TX + 32)
            const __grid_constant__ CUtensorMap tm_cf, const ShotDesc *__restrict__ shots, const int4 *__restrict__ prog,
            int L, int shot_base, int nshot, int chunk, int *err)
 {
-    tile_body<TX, NST, MATH, GPT, 1>(tm_p1, tm_p0, tm_cf, shots, prog, L, shot_base, nshot, chunk, err, blockIdx.y);
+    tile_body<TX, NST, MATH, GPT, 1>(tm_p1, tm_p0, tm_cf, shots, prog, L, shot_base, nshot, chunk, err, blockIdx.x,
+                                     blockIdx.y, blockIdx.z);
 }
 
 // the same step compiled for three blocks per SM, one group per thread, coefficients read from
@@ -620,14 +621,16 @@ __global__ void __launch_bounds__(TG * TX + 32, 3)
             const __grid_constant__ CUtensorMap tm_cf, const ShotDesc *__restrict__ shots, const int4 *__restrict__ prog,
             int L, int shot_base, int nshot, int chunk, int *err)
 {
-    tile_body<TX, NST, MATH, 1, 3>(tm_p1, tm_p0, tm_cf, shots, prog, L, shot_base, nshot, chunk, err, blockIdx.y);
+    tile_body<TX, NST, MATH, 1, 3>(tm_p1, tm_p0, tm_cf, shots, prog, L, shot_base, nshot, chunk, err, blockIdx.x,
+                                   blockIdx.y, blockIdx.z);
 }
 
 // ------------------------------------------------------------ several groups in one launch
 // One shot group of a launch that advances several independent runs at once (the continuous
 // batching of the request loop): its own tensor maps (in global memory), shots, program and the
-// launch index at which its program started.  Groups are stacked along grid y; a block finds its
-// group by its row, and blocks outside the group's tiles or program return at once.
+// launch index at which its program started.  The launch is a flat list of blocks: group g owns
+// blocks b0 .. b0 + nblk - 1, one per (column tile or receiver column, z tile, row), so no block
+// of the launch is idle by construction; a block finds its group by its index.
 struct __align__(128) TileGroup {
     CUtensorMap p1, p0, cf;       // as the single-group kernel's parameters
     const ShotDesc *shots;        // descriptors of the run's shots (shot_base .. shot_base + nshot - 1)
@@ -635,8 +638,9 @@ struct __align__(128) TileGroup {
     long long L0;                 // launch index of the program's item 0
     int nprog;                    // items of the program
     int shot_base, nshot, chunk;  // as the single-group kernel's parameters
-    int y0;                       // first grid row of the group (2 rows per chunk)
+    int b0, nblk;                 // first block and blocks of the group
     int ntx, zt;                  // column tiles (ntx: the receiver-sampling column) and z tiles
+    int halves;                   // 1: the program uses item halves .x only (forward); 2: both
 };
 
 template <int TX, int NST, int MATH>
@@ -644,17 +648,21 @@ __global__ void __launch_bounds__(TG * TX + 32, 3)
     k_tile_groups(const TileGroup *__restrict__ groups, int ngroups, long long L, int *err)
 {
     int g = 0;
-    while (g + 1 < ngroups && (int)blockIdx.y >= groups[g + 1].y0) ++g;
+    while (g + 1 < ngroups && (int)blockIdx.x >= groups[g + 1].b0) ++g;
     const TileGroup &T = groups[g];
     const long long Lg = L - T.L0;
-    if (Lg < 0 || Lg >= T.nprog || (int)blockIdx.x > T.ntx || (int)blockIdx.z >= T.zt) return;
+    if (Lg < 0 || Lg >= T.nprog) return;
+    const int l = (int)blockIdx.x - T.b0;
+    const int bx = l % (T.ntx + 1), rest = l / (T.ntx + 1);
+    const int bz = rest % T.zt, row = rest / T.zt;
+    const int by = T.halves == 2 ? row : 2 * row;
     // the maps live in global memory, written before the launch: make them visible to the
     // tensor-map proxy of this thread before its copies use them
     asm volatile("fence.proxy.tensormap::generic.acquire.gpu [%0], 128;" ::"l"(&T.p1) : "memory");
     asm volatile("fence.proxy.tensormap::generic.acquire.gpu [%0], 128;" ::"l"(&T.p0) : "memory");
     asm volatile("fence.proxy.tensormap::generic.acquire.gpu [%0], 128;" ::"l"(&T.cf) : "memory");
     tile_body<TX, NST, MATH, 1, 3>(T.p1, T.p0, T.cf, T.shots, T.prog, (int)Lg, T.shot_base, T.nshot, T.chunk, err,
-                                   (int)blockIdx.y - T.y0);
+                                   bx, by, bz);
 }
 
 }  // namespace fwi

@@ -389,7 +389,9 @@ FWI_API int fwi_l2_copy_probe(void *d_a, void *d_b, long long bytes, int passes,
 /* the launch program of one shot's adjoint pass (host-only, no device needed): four ints per
  * launch {kindA, stepA, kindB, stepB} with kinds 0 none, 3 replay step, 4 adjoint step.
  * overlap 0 is the reference's order (a segment is replayed when the reverse loop reaches it,
- * propagation.c:641-673); overlap 1 replays segment k-1 alongside the adjoint steps of segment k.
+ * propagation.c:641-673); overlap 1 replays segment k-1 alongside the adjoint steps of segment k;
+ * overlap 2 is the two-step kernel's program: as 1, with up to two replay and two adjoint steps
+ * per launch (a kind | 0x100 advances two steps from the step given).
  * Returns the number of launches; writes at most cap launches when items is not NULL. */
 FWI_API int fwi_adjoint_program(int nt, int overlap, int *items, int cap);
 /* checkpoint interval d = max(round(sqrt(2(nt-1))), 3) of checkpoint.c:47 */

@@ -1,8 +1,9 @@
-"""The TMA-fed step kernel in all of its launch shapes.
+"""The TMA-fed step kernels in all of their launch shapes.
 
-The engine picks the tile width (8 or 16 columns), the depth of the shared-memory stage
-ring (2 to 4 shots in flight) and the number of shots each block walks; environment
-variables override the choice.  Every shape must give the same bits: the reference's
+The engine advances two steps per launch by default (the two-step kernel, temporal blocking;
+FWI_DEPTH=1 selects the one-step kernel) and picks the tile width (8 or 16 columns, one-step
+kernel), the depth of the shared-memory stage ring (2 to 4 shots in flight) and the number of
+shots each block walks; environment variables override the choice.  Every shape must give the same bits: the reference's
 golden seismograms and gradient, and -- on a 12-shot survey where blocks walk more
 shots than the ring has stages -- the results of the previous cp.async kernel.  The
 contracted-FMA mode is held to the stated FP32 tolerance instead.
@@ -19,20 +20,27 @@ from golden_cases import Case
 pytestmark = pytest.mark.gpu
 
 SHAPES = [
+    # the two-step kernel (temporal blocking, the default)
     {},
-    {"FWI_TX": "8"},
-    {"FWI_TX": "16", "FWI_NST": "2", "FWI_CHUNK": "1"},
-    {"FWI_TX": "8", "FWI_NST": "2", "FWI_CHUNK": "3"},
-    {"FWI_TX": "16", "FWI_NST": "4", "FWI_CHUNK": "2"},
-    {"FWI_TX": "16", "FWI_NST": "3", "FWI_CHUNK": "32"},
-    {"FWI_GPT": "2"},
-    {"FWI_TX": "8", "FWI_GPT": "2", "FWI_NST": "3", "FWI_CHUNK": "5"},
-    {"FWI_TX": "16", "FWI_GPT": "2", "FWI_NST": "2", "FWI_CHUNK": "1"},
-    {"FWI_OCC": "3"},
-    {"FWI_OCC": "3", "FWI_NST": "3", "FWI_CHUNK": "8"},
-    {"FWI_OCC": "3", "FWI_NST": "2", "FWI_CHUNK": "1"},
+    {"FWI_NST": "3"},
+    {"FWI_NST": "2", "FWI_CHUNK": "1"},
+    {"FWI_NST": "3", "FWI_CHUNK": "5"},
+    {"FWI_NST": "2", "FWI_CHUNK": "32"},
+    # the one-step kernel in its launch shapes
+    {"FWI_DEPTH": "1"},
+    {"FWI_DEPTH": "1", "FWI_TX": "8"},
+    {"FWI_DEPTH": "1", "FWI_TX": "16", "FWI_NST": "2", "FWI_CHUNK": "1"},
+    {"FWI_DEPTH": "1", "FWI_TX": "8", "FWI_NST": "2", "FWI_CHUNK": "3"},
+    {"FWI_DEPTH": "1", "FWI_TX": "16", "FWI_NST": "4", "FWI_CHUNK": "2"},
+    {"FWI_DEPTH": "1", "FWI_TX": "16", "FWI_NST": "3", "FWI_CHUNK": "32"},
+    {"FWI_DEPTH": "1", "FWI_GPT": "2"},
+    {"FWI_DEPTH": "1", "FWI_TX": "8", "FWI_GPT": "2", "FWI_NST": "3", "FWI_CHUNK": "5"},
+    {"FWI_DEPTH": "1", "FWI_TX": "16", "FWI_GPT": "2", "FWI_NST": "2", "FWI_CHUNK": "1"},
+    {"FWI_DEPTH": "1", "FWI_OCC": "3"},
+    {"FWI_DEPTH": "1", "FWI_OCC": "3", "FWI_NST": "3", "FWI_CHUNK": "8"},
+    {"FWI_DEPTH": "1", "FWI_OCC": "3", "FWI_NST": "2", "FWI_CHUNK": "1"},
 ]
-KEYS = ("FWI_TX", "FWI_NST", "FWI_CHUNK", "FWI_KERNEL", "FWI_MATH", "FWI_TUNE", "FWI_GPT", "FWI_OCC")
+KEYS = ("FWI_TX", "FWI_NST", "FWI_CHUNK", "FWI_KERNEL", "FWI_MATH", "FWI_TUNE", "FWI_GPT", "FWI_OCC", "FWI_DEPTH")
 
 
 def rel(a, b):
@@ -174,7 +182,7 @@ def test_many_receivers_match_cp_async_kernel():
     assert all(len(s.igx) == nx for s in shots)  # a receiver in every column
     with env(FWI_KERNEL="step"):
         ref, _ = run_case(vp, rho, 10.0, 0.001, nt, 10, 1, shots)
-    for shape in ({}, {"FWI_OCC": "3"}, {"FWI_TX": "8"}):
+    for shape in ({}, {"FWI_DEPTH": "1"}, {"FWI_DEPTH": "1", "FWI_OCC": "3"}, {"FWI_DEPTH": "1", "FWI_TX": "8"}):
         with env(**shape):
             got, _ = run_case(vp, rho, 10.0, 0.001, nt, 10, 1, shots)
         for i, (a, b) in enumerate(zip(got, ref)):

@@ -30,3 +30,18 @@ def test_reduced_precision_snapshots_exceed_the_gradient_tolerance(port32, port6
     assert err["fp32"] < 1e-4  # what the engine stores
     assert 1e-4 < err["fp16"] < 2e-3  # FP16 (max-abs scaled): about its 2^-11 precision, above tolerance
     assert 1e-3 < err["bf16"] < 2e-2  # BF16: about its 2^-8 precision
+
+
+def test_large_grid_record():
+    """The same study on the precision-study grid (1201 x 4001 at 5 m, 20 Hz, nt = 8001; one shot of the
+    100-shot survey, run by tests/golden/precision_study.py with the oracle and its FP64 build): the
+    recorded errors keep FP32 snapshots within the gradient tolerance and put both reduced formats
+    above it; the FP32 seismogram stays within 1e-5 of the FP64 build."""
+    import json
+    import os
+    rec = json.load(open(os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden", "precision_config3.json")))
+    tol = rec["gradient_tolerance"]
+    assert rec["seismogram_fp32_rel_l2"] < 1e-5
+    assert rec["fp32"]["gradient_rel_l2"] < tol
+    assert rec["fp16_maxabs"]["gradient_rel_l2"] > tol and rec["bf16"]["gradient_rel_l2"] > tol
+    assert rec["fp32"]["steplen_rel"] < rec["fp16_maxabs"]["steplen_rel"]

@@ -3,10 +3,13 @@
 The engine keeps only the forward checkpoint pairs and rebuilds the other forward
 fields segment by segment (checkpoint.c:130-265, propagation.c:641-673).  With overlap,
 the rebuild of segment k-1 runs in the same launches as the adjoint steps of segment
-k.  This test replays a program symbolically: every frame buffer holds the time index
-of the field it contains, items of one launch read the state before the launch and
-write after it, and every read must find the field its step needs.  The buffer
-mapping below restates the device's (fwi_kernels.cuh: stored_slot, seg_buf, rep_buf).
+k.  The two-step kernel's program (overlap 2) advances up to two replay steps and two adjoint
+steps per launch.  This test replays a program symbolically: every frame buffer holds the
+time index of the field it contains, items of one launch read the state before the launch
+and write after it, every read must find the field its step needs, and no launch writes a
+buffer that it also reads (the blocks of a launch read halos of each other's inputs).  The
+buffer mapping below restates the device's (fwi_kernels.cuh: stored_slot, seg_idx, rep_idx,
+adj_idx; fields that are not kept rotate through four frames).
 """
 import ctypes as C
 
@@ -16,6 +19,8 @@ import pytest
 from fwiedu import engine as E
 
 K_NONE, K_REP, K_ADJ = 0, 3, 4
+DEPTH2 = 0x100
+NROT = 4
 
 
 def program(nt, overlap):
@@ -57,7 +62,10 @@ class Buffers:
             return ("ck", s)
         if t % 5 == 0:
             return self.seg(t)
-        return ("rscr", t % 3)
+        return ("rscr", t % NROT)
+
+    def adj(self, t):
+        return ("adj", (t + NROT) % NROT)
 
     def img(self, t):
         s = self.slot(t)
@@ -71,19 +79,27 @@ def simulate(nt, overlap):
         s = B.slot(t)
         if s >= 0:
             state[("ck", s)] = t
+    state[B.adj(nt)] = nt          # the adjoint pass starts from A(nt) = 0 and A(nt - 1)
+    state[B.adj(nt - 1)] = nt - 1
     adj_seen = []
     rep_seen = []
     for launch in program(nt, overlap):
         reads, writes = [], []
-        for kind, step in ((launch[0], launch[1]), (launch[2], launch[3])):
+        for kw, step in ((launch[0], launch[1]), (launch[2], launch[3])):
+            kind, steps = kw & 0xFF, (2 if kw & DEPTH2 else 1)
             if kind == K_REP:
                 reads += [(B.rep(step), step), (B.rep(step - 1), step - 1)]
-                writes.append((B.rep(step + 1), step + 1))
-                rep_seen.append(step)
+                for j in range(steps):
+                    writes.append((B.rep(step + 1 + j), step + 1 + j))
+                    rep_seen.append(step + j)
             elif kind == K_ADJ:
-                if step % 5 == 0:
-                    reads.append((B.img(step), step))
-                adj_seen.append(step)
+                reads += [(B.adj(step), step), (B.adj(step + 1), step + 1)]
+                for j in range(steps):
+                    t = step - j
+                    if t % 5 == 0:
+                        reads.append((B.img(t), t))
+                    writes.append((B.adj(t - 1), t - 1))
+                    adj_seen.append(t)
             else:
                 assert kind == K_NONE
         for buf, want in reads:
@@ -97,7 +113,7 @@ def simulate(nt, overlap):
 
 
 @pytest.mark.parametrize("nt", [1, 2, 3, 4, 7, 10, 37, 100, 200, 201, 299, 300, 451, 1000, 4001])
-@pytest.mark.parametrize("overlap", [0, 1])
+@pytest.mark.parametrize("overlap", [0, 1, 2])
 def test_program_feeds_every_imaging_step(nt, overlap):
     adj, rep, B = simulate(nt, overlap)
     assert adj == list(range(nt - 1, -1, -1))
@@ -112,3 +128,10 @@ def test_overlap_removes_most_replay_launches():
     over = len(program(nt, 1))
     assert plain == nt + (nt - 89)  # the reference's 3912 replay steps, one launch each
     assert over < nt + 2 * 89  # replay hidden behind the adjoint steps except the last segment
+
+
+def test_two_step_program_halves_the_launches():
+    nt = 4001
+    one = len(program(nt, 1))
+    two = len(program(nt, 2))
+    assert two < 0.55 * one
