@@ -507,23 +507,25 @@ def plain_path(E, local, vp, rho, vp0, rho0, shots, obs, reps=2):
         ctx.set_model(vp, rho, DX, DX, DT, NT, PML, FS)
         fms = fcells = 0.0
         flaunch = 0
+        fpass = 0.0
         for r in range(reps + 1):
             ctx.run(0, path=E.PATH_PLAIN)
-            st = ctx.stats()
+            st, ps = ctx.stats(), ctx.pass_stats()
             if r:
                 fms += st["ms"]
+                fpass += ps["fwd_ms"]
                 fcells += st["cell_updates"]
-                flaunch += st["kernel_launches"]
+                flaunch += ps["fwd_launches"]
     finally:
         ctx.close()
     l2 = l2_peak_gbs(local)
     # one step launch of one shot: 12 B of fields + 24 B of its own coefficient planes per cell
     bpc = 36.0
-    achieved = fcells * bpc / (fms * 1e-3) / 1e9
+    achieved = fcells * bpc / (fpass * 1e-3) / 1e9  # the step launches' own time
     return {"shot_gradients_per_s": sgps, "gcells_per_s": gcells,
             "forward_shots_per_s": len(sh) * reps / (fms / 1e3), "forward_gcells_per_s": fcells / (fms * 1e6),
             "roofline": {"bound": "l2", "achieved": achieved, "peak": l2, "unit": "GB/s", "frac": achieved / l2,
-                         "bytes_per_cell_update": bpc, "launch_us": fms * 1e3 / max(flaunch, 1),
+                         "bytes_per_cell_update": bpc, "launch_us": fpass * 1e3 / max(flaunch, 1),
                          "peak_source": "measured in this run: L2-resident copy, fwi_l2_copy_probe"},
             "sample": f"shots {idx} of the survey, {reps} timed runs after one untimed (autotuner) run",
             "note": "one shot per launch; gradient figure = problem 1 + problem 2 (the iteration's engine work)"}
@@ -534,31 +536,35 @@ TRAFFIC = os.path.join(ROOT, "profiles", "k_tile_forward_60shots_traffic.json")
 
 
 def step_roofline(ctx, E, peaks):
-    """Time the fused step kernel alone: the batched forward pass (one k_tile launch per time
-    step, all 60 shots per launch), device time from CUDA events on the engine's stream.
-    `traffic` is the DRAM read + write of one such launch from the committed ncu capture of the
-    same launch (60 shots of the 221 x 601 survey, the size this bench runs)."""
+    """Time the fused step kernel alone: the batched forward pass (all 60 shots in every launch;
+    the two-step kernel advances them two steps per launch), device time of the pass from the
+    engine's CUDA events around it.  Algorithmic bytes per cell-update with S shots stepping
+    together on one coefficient set: p1 read + p0 read + p2 write (12 B) + 6 coefficient planes
+    read once for the S shots (24 B / S), whatever the kernel moves.  `traffic` is the DRAM read
+    + write of one launch from the committed ncu capture of the same launch."""
     ctx.run(0, path=E.PATH_BATCHED)
     ctx.run(0, path=E.PATH_BATCHED)
-    st = ctx.stats()
-    per_launch_ms = st["ms"] / st["kernel_launches"]
+    st, ps = ctx.stats(), ctx.pass_stats()
     shape = ctx.launch_shape()
-    cells_per_launch = st["cell_updates"] / NT
-    # algorithmic bytes per cell-update with S shots stepping together on one coefficient set:
-    # p1 read + p0 read + p2 write (12 B) + 6 coefficient planes read once for the S shots (24 B / S)
     S = NSHOT
     bpc = 12.0 + 24.0 / S
+    launches = max(ps["fwd_launches"], 1)
+    per_launch_ms = ps["fwd_ms"] / launches
+    steps_per_launch = NT / launches
+    cells_per_launch = st["cell_updates"] / launches
     bytes_per_launch = cells_per_launch * bpc
     achieved = bytes_per_launch / (per_launch_ms * 1e-3) / 1e9
     peak = peaks.get("hbm_gbs")
-    traffic = None
+    traffic = tinfo = None
     if os.path.exists(TRAFFIC):
-        t = json.load(open(TRAFFIC))
-        traffic = t["dram_read_bytes"] + t["dram_write_bytes"]
+        tinfo = json.load(open(TRAFFIC))
+        traffic = tinfo["dram_read_bytes"] + tinfo["dram_write_bytes"]
     return {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
             "frac": achieved / peak if peak else None, "traffic": traffic,
             "traffic_vs_algorithmic": traffic / bytes_per_launch if traffic else None,
-            "kernel": "k_tile (batched forward, 60 shots per launch)",
+            "traffic_source": tinfo.get("kernel") if tinfo else None,
+            "kernel": "step kernel (batched forward, 60 shots per launch)",
+            "steps_per_launch": steps_per_launch,
             "launch_us": per_launch_ms * 1e3, "gcells_per_s": cells_per_launch / (per_launch_ms * 1e-3) / 1e9,
             "bytes_per_cell_update": bpc, "algorithmic_bytes_per_launch": bytes_per_launch,
             "shots_sharing_coefficients": S, "peak_source": "fallback" if peaks.get("fallback") else "measured",

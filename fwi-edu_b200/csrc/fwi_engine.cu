@@ -140,7 +140,7 @@ struct fwi_ctx {
     std::map<std::string, cudaGraphExec_t> graphs;
     fwi_stats stats{};
     int math = 0;  // 0: bit-exact arithmetic, 1: contracted multiply-adds
-    int depth = 2;  // time steps per launch of the step kernel (1 or 2; FWI_DEPTH)
+    int depth = 1;  // time steps per launch of the step kernel (1 or 2; FWI_DEPTH)
     bool use_graphs = true;  // capture the batched launch sequences as CUDA graphs
     bool pdl = true;         // consecutive steps as programmatic dependent launches
     bool tune = true;        // time the step kernel's launch shapes once per shape (autotune)
@@ -247,7 +247,7 @@ extern "C" int fwi_ctx_create(fwi_ctx **out, int device, size_t budget)
     c->device = device;
     c->budget = budget;
     if (const char *e = getenv("FWI_MATH")) c->math = atoi(e) ? 1 : 0;
-    if (const char *e = getenv("FWI_DEPTH")) c->depth = atoi(e) == 1 ? 1 : 2;
+    if (const char *e = getenv("FWI_DEPTH")) c->depth = atoi(e) == 2 ? 2 : 1;
     if (const char *e = getenv("FWI_GRAPH")) c->use_graphs = e[0] != '0';  // 0: direct launches (profilers)
     if (const char *e = getenv("FWI_PDL")) c->pdl = e[0] != '0';
     if (const char *e = getenv("FWI_TUNE")) c->tune = e[0] != '0';            // 0: heuristic launch shapes

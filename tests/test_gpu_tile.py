@@ -1,7 +1,7 @@
 """The TMA-fed step kernels in all of their launch shapes.
 
-The engine advances two steps per launch by default (the two-step kernel, temporal blocking;
-FWI_DEPTH=1 selects the one-step kernel) and picks the tile width (8 or 16 columns, one-step
+The engine advances one step per launch by default (FWI_DEPTH=2 selects the two-step kernel,
+temporal blocking) and picks the tile width (8 or 16 columns, one-step
 kernel), the depth of the shared-memory stage ring (2 to 4 shots in flight) and the number of
 shots each block walks; environment variables override the choice.  Every shape must give the same bits: the reference's
 golden seismograms and gradient, and -- on a 12-shot survey where blocks walk more
@@ -20,12 +20,13 @@ from golden_cases import Case
 pytestmark = pytest.mark.gpu
 
 SHAPES = [
-    # the two-step kernel (temporal blocking, the default)
+    # the one-step kernel (the default) and the two-step kernel (temporal blocking)
     {},
-    {"FWI_NST": "3"},
-    {"FWI_NST": "2", "FWI_CHUNK": "1"},
-    {"FWI_NST": "3", "FWI_CHUNK": "5"},
-    {"FWI_NST": "2", "FWI_CHUNK": "32"},
+    {"FWI_DEPTH": "2"},
+    {"FWI_DEPTH": "2", "FWI_NST": "3"},
+    {"FWI_DEPTH": "2", "FWI_NST": "2", "FWI_CHUNK": "1"},
+    {"FWI_DEPTH": "2", "FWI_NST": "3", "FWI_CHUNK": "5"},
+    {"FWI_DEPTH": "2", "FWI_NST": "2", "FWI_CHUNK": "32"},
     # the one-step kernel in its launch shapes
     {"FWI_DEPTH": "1"},
     {"FWI_DEPTH": "1", "FWI_TX": "8"},
@@ -182,7 +183,7 @@ def test_many_receivers_match_cp_async_kernel():
     assert all(len(s.igx) == nx for s in shots)  # a receiver in every column
     with env(FWI_KERNEL="step"):
         ref, _ = run_case(vp, rho, 10.0, 0.001, nt, 10, 1, shots)
-    for shape in ({}, {"FWI_DEPTH": "1"}, {"FWI_DEPTH": "1", "FWI_OCC": "3"}, {"FWI_DEPTH": "1", "FWI_TX": "8"}):
+    for shape in ({}, {"FWI_DEPTH": "2"}, {"FWI_DEPTH": "1", "FWI_OCC": "3"}, {"FWI_DEPTH": "1", "FWI_TX": "8"}):
         with env(**shape):
             got, _ = run_case(vp, rho, 10.0, 0.001, nt, 10, 1, shots)
         for i, (a, b) in enumerate(zip(got, ref)):
