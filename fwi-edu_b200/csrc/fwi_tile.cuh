@@ -77,16 +77,41 @@ __device__ __forceinline__ u64 fma2(u64 a, u64 b, u64 c)
     return d;
 }
 
-// stencil constants (propagation.h) and grid spacings as packed pairs.  The exact path rounds
-// every product on its own with two scalar multiplies (__fmul_rn is never contracted); a
-// packed multiply would be fused by the compiler into the following packed add (one rounding
-// instead of two) although both carry .rn.  The sums stay packed.
+// stencil constants (propagation.h)
+constexpr float FD_C1 = 0.77793115f, FD_C2 = -0.17388691f, FD_C3 = 0.02338713f;
+constexpr float FD_D0 = -2.8215452f, FD_D1 = 1.57663238f, FD_D2 = -0.18347238f, FD_D3 = 0.01761260f;
+
+// the stencil constants and grid spacings as packed pairs (the contracted path), and the spacings
+// as scalars (the exact path, whose products are scalar multiplies: the constants enter them as
+// immediates and hold no registers)
 struct PkConst {
     u64 C1, C2, C3, D0, D1, D2, D3, idx, idz, idxx, idzz;
+    float sidxx, sidzz;
 };
+__device__ __forceinline__ PkConst make_pkconst(float invdx, float invdz, float invdxdx, float invdzdz)
+{
+    PkConst K;
+    K.C1 = pk(FD_C1, FD_C1);
+    K.C2 = pk(FD_C2, FD_C2);
+    K.C3 = pk(FD_C3, FD_C3);
+    K.D0 = pk(FD_D0, FD_D0);
+    K.D1 = pk(FD_D1, FD_D1);
+    K.D2 = pk(FD_D2, FD_D2);
+    K.D3 = pk(FD_D3, FD_D3);
+    K.idx = pk(invdx, invdx);
+    K.idz = pk(invdz, invdz);
+    K.idxx = pk(invdxdx, invdxdx);
+    K.idzz = pk(invdzdz, invdzdz);
+    K.sidxx = invdxdx;
+    K.sidzz = invdzdz;
+    return K;
+}
 
-// two vertically adjacent cells of one column: propagation.c:13-74 with each product and
-// sum rounded on its own, in the reference's order
+// Two vertically adjacent cells of one column: propagation.c:13-74 with each product and sum
+// rounded on its own, in the reference's order.  The exact path (MATH 0) rounds every product
+// on its own with two scalar multiplies (__fmul_rn is never contracted; a packed multiply would
+// be fused by the compiler into the following packed add although both carry .rn); the sums stay
+// packed.
 template <int MATH>
 __device__ __forceinline__ u64 cell2(u64 zm3, u64 zm2, u64 zm1, u64 z0, u64 zp1, u64 zp2, u64 zp3, u64 xm3, u64 xm2,
                                      u64 xm1, u64 xp1, u64 xp2, u64 xp3, u64 c1, u64 c2, u64 ck, u64 irx, u64 irz,
@@ -97,18 +122,22 @@ __device__ __forceinline__ u64 cell2(u64 zm3, u64 zm2, u64 zm1, u64 z0, u64 zp1,
             const float2 x = upk(a), y = upk(b);
             return pk(__fmul_rn(x.x, y.x), __fmul_rn(x.y, y.y));
         };
+        auto mulk = [&](float c, u64 b) {
+            const float2 y = upk(b);
+            return pk(__fmul_rn(c, y.x), __fmul_rn(c, y.y));
+        };
         // dpdz and dpdx feed multiplies only: a packed multiply there cannot be fused into an add
         const u64 dpdz =
-            mul2(add2(add2(mul(k.C1, sub2(zp1, zm1)), mul(k.C2, sub2(zp2, zm2))), mul(k.C3, sub2(zp3, zm3))), k.idz);
+            mul2(add2(add2(mulk(FD_C1, sub2(zp1, zm1)), mulk(FD_C2, sub2(zp2, zm2))), mulk(FD_C3, sub2(zp3, zm3))),
+                 k.idz);
         const u64 dpdx =
-            mul2(add2(add2(mul(k.C1, sub2(xp1, xm1)), mul(k.C2, sub2(xp2, xm2))), mul(k.C3, sub2(xp3, xm3))), k.idx);
-        const u64 d0 = mul(k.D0, z0);
-        const u64 dzz =
-            mul(add2(add2(add2(d0, mul(k.D1, add2(zp1, zm1))), mul(k.D2, add2(zp2, zm2))), mul(k.D3, add2(zp3, zm3))),
-                k.idzz);
-        const u64 dxx =
-            mul(add2(add2(add2(d0, mul(k.D1, add2(xp1, xm1))), mul(k.D2, add2(xp2, xm2))), mul(k.D3, add2(xp3, xm3))),
-                k.idxx);
+            mul2(add2(add2(mulk(FD_C1, sub2(xp1, xm1)), mulk(FD_C2, sub2(xp2, xm2))), mulk(FD_C3, sub2(xp3, xm3))),
+                 k.idx);
+        const u64 d0 = mulk(FD_D0, z0);
+        const u64 dzz = mulk(k.sidzz, add2(add2(add2(d0, mulk(FD_D1, add2(zp1, zm1))), mulk(FD_D2, add2(zp2, zm2))),
+                                           mulk(FD_D3, add2(zp3, zm3))));
+        const u64 dxx = mulk(k.sidxx, add2(add2(add2(d0, mulk(FD_D1, add2(xp1, xm1))), mulk(FD_D2, add2(xp2, xm2))),
+                                           mulk(FD_D3, add2(xp3, xm3))));
         const u64 lap = add2(add2(mul(irx, dpdx), mul(irz, dpdz)), mul(ir, add2(dxx, dzz)));
         return add2(add2(mul(c1, z0), mul(c2, p0)), mul(ck, lap));
     } else {
@@ -420,18 +449,7 @@ __device__ __forceinline__ void tile_body(const CUtensorMap &tm_p1, const CUtens
     const bool acc_tile = hess || image;
     const long long colx = (long long)x * A.ld;
     const float invdx = A.invdx, invdz = A.invdz, invdtdt = A.invdtdt;
-    PkConst K;
-    K.C1 = pk(0.77793115f, 0.77793115f);
-    K.C2 = pk(-0.17388691f, -0.17388691f);
-    K.C3 = pk(0.02338713f, 0.02338713f);
-    K.D0 = pk(-2.8215452f, -2.8215452f);
-    K.D1 = pk(1.57663238f, 1.57663238f);
-    K.D2 = pk(-0.18347238f, -0.18347238f);
-    K.D3 = pk(0.01761260f, 0.01761260f);
-    K.idx = pk(invdx, invdx);
-    K.idz = pk(invdz, invdz);
-    K.idxx = pk(A.invdxdx, A.invdxdx);
-    K.idzz = pk(A.invdzdz, A.invdzdz);
+    const PkConst K = make_pkconst(invdx, invdz, A.invdxdx, A.invdzdz);
     const float4 zero4 = make_float4(0.f, 0.f, 0.f, 0.f);
     const float4(*scf)[TX][TG] = reinterpret_cast<const float4(*)[TX][TG]>(smem);
     constexpr bool CF_REG = GPT == 1 && MINB < 3;
@@ -550,7 +568,6 @@ __device__ __forceinline__ void tile_body(const CUtensorMap &tm_p1, const CUtens
         }
     };
 
-    // one shot of the chunk from ring stage st: the lane's GPT groups, sharing their z-window
     // one shot of the chunk from ring stage st: the lane's GPT groups, sharing their z-window;
     // FAST: the store-only epilogue
     auto consume_shot = [&](int i, int st, auto fast) {

@@ -175,18 +175,7 @@ __global__ void __launch_bounds__(TG * TX + 32, 2)
     const int zlo = A.izStart, zhi = Nz - 4;
     const int fs_hi = min(2 * pml, pml + 3);  // last mirrored source row (snapshot steps use the one-step kernel)
     const float invdx = A.invdx, invdz = A.invdz, invdtdt = A.invdtdt;
-    PkConst K;
-    K.C1 = pk(0.77793115f, 0.77793115f);
-    K.C2 = pk(-0.17388691f, -0.17388691f);
-    K.C3 = pk(0.02338713f, 0.02338713f);
-    K.D0 = pk(-2.8215452f, -2.8215452f);
-    K.D1 = pk(1.57663238f, 1.57663238f);
-    K.D2 = pk(-0.18347238f, -0.18347238f);
-    K.D3 = pk(0.01761260f, 0.01761260f);
-    K.idx = pk(invdx, invdx);
-    K.idz = pk(invdz, invdz);
-    K.idxx = pk(A.invdxdx, A.invdxdx);
-    K.idzz = pk(A.invdzdz, A.invdzdz);
+    const PkConst K = make_pkconst(invdx, invdz, A.invdxdx, A.invdzdz);
     const float4 zero4 = make_float4(0.f, 0.f, 0.f, 0.f);
     // shared-memory addresses: coefficient plane f, grown-region column c, group g
     auto cf_at = [&](int f, int c, int g) { return sm0 + (unsigned)(((f * Geo::CX + c) * Geo::CG + g) * 16); };
