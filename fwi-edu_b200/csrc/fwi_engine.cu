@@ -42,6 +42,7 @@
 #include "fwi_step.cuh"
 #include "fwi_tile.cuh"
 #include "fwi_tile2.cuh"
+#include "fwi_wave.cuh"
 #include "fwi_optim.cuh"
 #include "fwi_fft.cuh"
 
@@ -144,7 +145,12 @@ struct fwi_ctx {
     bool use_graphs = true;  // capture the batched launch sequences as CUDA graphs
     bool pdl = true;         // consecutive steps as programmatic dependent launches
     bool tune = true;        // time the step kernel's launch shapes once per shape (autotune)
+    bool wave = true;        // forward passes as one persistent wavefront launch where they fit (FWI_WAVE)
+    int *d_wave = nullptr;   // its abort word and per-block item counters
+    int wave_cap = 0;
+    std::map<std::string, long long> graph_launches;  // kernels each captured graph holds
     int last_tx = 0, last_nst = 0, last_chunk = 0, last_gpt = 0, last_minb = 0;  // the shape of the last launch
+    bool last_wave = false;  // the last pass ran as one persistent wavefront launch
     int *d_err = nullptr;  // set by a step kernel whose tile copy did not complete
     std::map<void *, size_t> sizes;  // live device blocks of this context
     size_t peak = 0;
@@ -256,6 +262,9 @@ extern "C" int fwi_ctx_create(fwi_ctx **out, int device, size_t budget)
     CK(cudaEventCreate(&c->ev1));
     TRY(dmalloc(c, (void **)&c->d_err, sizeof(int)));
     CK(cudaMemset(c->d_err, 0, sizeof(int)));
+    if (const char *e = getenv("FWI_WAVE")) c->wave = e[0] != '0';  // 0: forward passes as step launches
+    c->wave_cap = 4096;  // abort word + one counter per resident block (148 SMs x a few blocks)
+    TRY(dmalloc(c, (void **)&c->d_wave, c->wave_cap * sizeof(int)));
     *out = c;
     return FWI_OK;
 }
@@ -877,7 +886,7 @@ static LaunchCfg pick_launch(int Nx, int nshot, bool batched, int math)
 }
 
 typedef void (*TileFn)(const CUtensorMap, const CUtensorMap, const CUtensorMap, const ShotDesc *, const int4 *, int,
-                       int, int, int, int *);
+                       int, int, int, int, int *);
 
 template <int TX, int NST, int MATH, int GPT, int MINB>
 static TileFn tile_fn()
@@ -1005,7 +1014,11 @@ static int launch_tiles(fwi_ctx *c, const Program *prog, int L0, int L1, int sho
                          : (c->math ? tile_fn_gpt<8, 1>(nst, gpt, minb) : tile_fn_gpt<8, 0>(nst, gpt, minb));
     const int smem = tx == 16 ? TileGeom<16>::smem(nst) : TileGeom<8>::smem(nst);
     const int ntx = (p->Nx + tx - 1) / tx, nchunks = (nshot + chunk - 1) / chunk;
-    dim3 grid(ntx + 1, 2 * nchunks, zt);
+    // items whose second half is empty throughout (a forward pass) need no blocks for it
+    int halves = 1;
+    for (int L = L0; L < L1 && halves == 1; L++)
+        if (prog->items[L].z != K_NONE) halves = 2;
+    dim3 grid(ntx + 1, halves * nchunks, zt);
     CUtensorMap m1, m0, mc;
     if (tx == 16) TRY(encode_group_maps<16>(r0->d, nshot, p->d_coef, &m1, &m0, &mc));
     else TRY(encode_group_maps<8>(r0->d, nshot, p->d_coef, &m1, &m0, &mc));
@@ -1025,7 +1038,7 @@ static int launch_tiles(fwi_ctx *c, const Program *prog, int L0, int L1, int sho
         const int4 &pw = prog->items[L];
         if (pw.x == K_NONE && pw.z == K_NONE) continue;
         CK(cudaLaunchKernelEx(&lc, fn, m1, m0, mc, (const ShotDesc *)c->d_desc, (const int4 *)prog->d, L, shot_base,
-                              nshot, chunk, c->d_err));
+                              nshot, chunk, halves, c->d_err));
         c->launches++;
         if (c->snapping) TRY(snapshots_after(c, prog, L, shot_base, nshot));
     }
@@ -1068,6 +1081,7 @@ static TileCfg tile_config(fwi_ctx *c, const Plan *p, int nshot, bool batched, i
     c->last_chunk = cfg.chunk;
     c->last_gpt = cfg.gpt;
     c->last_minb = cfg.minb;
+    c->last_wave = false;
     return cfg;
 }
 
@@ -1158,8 +1172,97 @@ static int autotune(fwi_ctx *c, int shot_base, int nshot, const ShotRun *r0, boo
     return FWI_OK;
 }
 
+// ---------------------------------------------------------------- persistent forward launch
+// Blocks of k_wave one SM holds at once (the launch is cooperative: every block resident).
+template <int NST, int MATH>
+static int wave_resident()
+{
+    static const int nb = [] {
+        auto f = k_wave<NST, MATH>;
+        const int smem = TileGeom<WAVE_TX>::smem(NST);
+        cudaFuncSetAttribute((const void *)f, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+        cudaFuncSetAttribute((const void *)f, cudaFuncAttributePreferredSharedMemoryCarveout,
+                             cudaSharedmemCarveoutMaxShared);
+        int b = 0;
+        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, f, TG * (WAVE_TX + 32 / TG), smem) != cudaSuccess) b = 0;
+        return b;
+    }();
+    return nb;
+}
+
+static constexpr int WAVE_NST = 4;
+
+// The wavefront launch's shape for items L0 .. L1-1 of a program over nshot shots of one group,
+// or false where it does not apply: the items must be consecutive forward steps, the run must
+// not write snapshots (the host copies them out between steps), and one block per 16-column
+// tile and shot range of 2 to WAVE_CH_MAX shots must fit the resident blocks.
+static bool wave_shape(fwi_ctx *c, const Program *prog, int L0, int L1, int nshot, const ShotRun *r0, int *ranges,
+                       int *per_range)
+{
+    const char *ke = getenv("FWI_KERNEL");
+    if (!c->wave || c->snapping || prog->depth != 1 || L1 <= L0 || nshot < 2 || (ke && strcmp(ke, "step") == 0))
+        return false;
+    for (int L = L0; L < L1; L++) {
+        const int4 &pw = prog->items[L];
+        if ((pw.x != K_FWD0 && pw.x != K_FWD1) || pw.z != K_NONE || pw.y != prog->items[L0].y + (L - L0)) return false;
+    }
+    const Plan *p = r0->plan;
+    const int tiles = ((p->Nx + WAVE_TX - 1) / WAVE_TX) * ((p->G + TG - 1) / TG);
+    int sms = 0;
+    if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, c->device) != cudaSuccess) return false;
+    const int slots = sms * (c->math ? wave_resident<WAVE_NST, 1>() : wave_resident<WAVE_NST, 0>());
+    if (tiles > slots) return false;
+    for (int nr = std::min(slots / tiles, nshot / 2); nr >= 1; --nr) {
+        const int n = (nshot + nr - 1) / nr;
+        if (n <= WAVE_CH_MAX && nshot - (nr - 1) * n >= 2 && tiles * nr + 1 <= c->wave_cap) {
+            *ranges = nr;
+            *per_range = n;
+            return true;
+        }
+    }
+    return false;
+}
+
+// the whole forward program as one launch of k_wave (fwi_wave.cuh)
+static int launch_wave(fwi_ctx *c, const Program *prog, int L0, int L1, int shot_base, int nshot, const ShotRun *r0,
+                       int nranges, int n)
+{
+    const Plan *p = r0->plan;
+    const int ntx = (p->Nx + WAVE_TX - 1) / WAVE_TX, zt = (p->G + TG - 1) / TG;
+    const int blocks = ntx * zt * nranges;
+    CUtensorMap m1, m0, mc;
+    TRY(encode_group_maps<WAVE_TX>(r0->d, nshot, p->d_coef, &m1, &m0, &mc));
+    CK(cudaMemsetAsync(c->d_wave, 0, (size_t)(blocks + 1) * sizeof(int), c->stream));
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeCooperative;
+    attr[0].val.cooperative = 1;
+    cudaLaunchConfig_t lc = {};
+    lc.gridDim = dim3(blocks);
+    lc.blockDim = dim3(TG, WAVE_TX + 32 / TG);
+    lc.dynamicSmemBytes = TileGeom<WAVE_TX>::smem(WAVE_NST);
+    lc.stream = c->stream;
+    lc.attrs = attr;
+    lc.numAttrs = 1;
+    auto fn = c->math ? k_wave<WAVE_NST, 1> : k_wave<WAVE_NST, 0>;
+    CK(cudaLaunchKernelEx(&lc, fn, m1, m0, mc, (const ShotDesc *)c->d_desc, (const int4 *)prog->d, L0, L1, shot_base,
+                          nshot, n, ntx, zt, nranges, c->d_wave, c->d_err));
+    c->launches++;
+    c->last_tx = WAVE_TX;
+    c->last_nst = WAVE_NST;
+    c->last_chunk = n;
+    c->last_gpt = 1;
+    c->last_minb = c->math ? wave_resident<WAVE_NST, 1>() : wave_resident<WAVE_NST, 0>();
+    c->last_wave = true;
+    return FWI_OK;
+}
+
 static int launch_steps(fwi_ctx *c, const Program *prog, int shot_base, int nshot, const ShotRun *r0, bool batched)
 {
+    {
+        int nranges = 0, n = 0;
+        if (batched && wave_shape(c, prog, 0, (int)prog->items.size(), nshot, r0, &nranges, &n))
+            return launch_wave(c, prog, 0, (int)prog->items.size(), shot_base, nshot, r0, nranges, n);
+    }
     const Plan *p = r0->plan;
     const int zt = (p->G + TG - 1) / TG;
     const int n = (int)prog->items.size();
@@ -1820,6 +1923,11 @@ static int run_program(fwi_ctx *c, const std::string &key, const Program *prog, 
     }
     if (!batched) return launch_steps(c, prog, shot_base, nshot, r0, false);
     if (!c->use_graphs) return launch_steps(c, prog, shot_base, nshot, r0, true);
+    {  // one wavefront launch needs no graph
+        int wr = 0, wn = 0;
+        if (wave_shape(c, prog, 0, (int)prog->items.size(), nshot, r0, &wr, &wn))
+            return launch_steps(c, prog, shot_base, nshot, r0, true);
+    }
     const std::string gk = key + "#" + std::to_string(prog->depth);  // graphs of one- and two-step programs differ
     auto it = c->graphs.find(gk);
     if (it == c->graphs.end()) {
@@ -1834,14 +1942,13 @@ static int run_program(fwi_ctx *c, const std::string &key, const Program *prog, 
         e = cudaGraphInstantiate(&ge, g, 0);
         cudaGraphDestroy(g);
         if (e != cudaSuccess) return fail(FWI_ERR_CUDA, "graph instantiate: %s", cudaGetErrorString(e));
+        c->graph_launches[gk] = c->launches - before;  // the kernels the graph holds
         c->launches = before;
         it = c->graphs.emplace(gk, ge).first;
     }
     CK(cudaGraphLaunch(it->second, c->stream));
     c->stats.graph_launches++;
-    // count the kernels the graph holds
-    for (const int4 &pw : prog->items)
-        if (pw.x != K_NONE || pw.z != K_NONE) c->launches++;
+    c->launches += c->graph_launches[gk];
     return FWI_OK;
 }
 
@@ -2207,6 +2314,13 @@ extern "C" int fwi_ctx_launch_variant(fwi_ctx *c, int *groups_per_thread, int *b
     if (!c) return fail(FWI_ERR_ARG, "ctx is NULL");
     if (groups_per_thread) *groups_per_thread = c->last_gpt;
     if (blocks_per_sm) *blocks_per_sm = c->last_minb;
+    return FWI_OK;
+}
+
+extern "C" int fwi_ctx_launch_persistent(fwi_ctx *c, int *persistent)
+{
+    if (!c) return fail(FWI_ERR_ARG, "ctx is NULL");
+    if (persistent) *persistent = c->last_wave ? 1 : 0;
     return FWI_OK;
 }
 

@@ -57,7 +57,9 @@ struct fwi_exec {
     long long launches_total = 0;
 };
 
-static const int EXEC_TX = 16, EXEC_NST = 3;
+// 16-column tiles, a ring of four stages (the depth the autotuner picks for large batches; the
+// three-stage build of the three-blocks-per-SM body spills more registers)
+static const int EXEC_TX = 16, EXEC_NST = 4;
 
 // the batched path's set-up of a run without waves: per-shot runs, groups of consecutive shots
 // sharing a model window, their frame pools and descriptors; initial frames zeroed
@@ -294,10 +296,12 @@ static int exec_fail_all(fwi_exec *ex, int code, const char *why)
     return fail(code, "%s", why);
 }
 
-// keep at most 64 launches in flight; read the error word as the device catches up
+// keep at most 128 launches in flight; read the error word as the device catches up.  The copy
+// and the event between two launches end the programmatic overlap of that pair, so they come
+// once per 32 launches.
 static int exec_throttle(fwi_exec *ex)
 {
-    if (ex->L % 8 != 0) return FWI_OK;
+    if (ex->L % 32 != 0) return FWI_OK;
     cudaEvent_t e;
     if (!ex->spare.empty()) {
         e = ex->spare.back();
@@ -308,7 +312,7 @@ static int exec_throttle(fwi_exec *ex)
     CK(cudaMemcpyAsync(ex->h_err, ex->d_err, sizeof(int), cudaMemcpyDeviceToHost, ex->stream));
     CK(cudaEventRecord(e, ex->stream));
     ex->inflight.push_back(e);
-    while (ex->inflight.size() > 8) {
+    while (ex->inflight.size() > 4) {
         CK(cudaEventSynchronize(ex->inflight.front()));
         ex->spare.push_back(ex->inflight.front());
         ex->inflight.pop_front();

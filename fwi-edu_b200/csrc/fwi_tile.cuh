@@ -620,14 +620,16 @@ __device__ __forceinline__ void tile_body(const CUtensorMap &tm_p1, const CUtens
 
 // the step kernel; the tensor maps are kernel parameters in constant space (the body takes
 // their addresses)
+// halves: 2 -- grid row y is 2 * chunk + item half; 1 -- the items' second halves are empty and
+// row y is the chunk (its first half)
 template <int TX, int NST, int MATH, int GPT>
 __global__ void __launch_bounds__(TG / GPT * TX + 32)
     k_tile(const __grid_constant__ CUtensorMap tm_p1, const __grid_constant__ CUtensorMap tm_p0,
            const __grid_constant__ CUtensorMap tm_cf, const ShotDesc *__restrict__ shots, const int4 *__restrict__ prog,
-           int L, int shot_base, int nshot, int chunk, int *err)
+           int L, int shot_base, int nshot, int chunk, int halves, int *err)
 {
     tile_body<TX, NST, MATH, GPT, 1>(tm_p1, tm_p0, tm_cf, shots, prog, L, shot_base, nshot, chunk, err, blockIdx.x,
-                                     blockIdx.y, blockIdx.z);
+                                     halves == 2 ? blockIdx.y : 2 * blockIdx.y, blockIdx.z);
 }
 
 // the same step compiled for three blocks per SM, one group per thread, coefficients read from
@@ -636,10 +638,10 @@ template <int TX, int NST, int MATH>
 __global__ void __launch_bounds__(TG * TX + 32, 3)
     k_tile3(const __grid_constant__ CUtensorMap tm_p1, const __grid_constant__ CUtensorMap tm_p0,
             const __grid_constant__ CUtensorMap tm_cf, const ShotDesc *__restrict__ shots, const int4 *__restrict__ prog,
-            int L, int shot_base, int nshot, int chunk, int *err)
+            int L, int shot_base, int nshot, int chunk, int halves, int *err)
 {
     tile_body<TX, NST, MATH, 1, 3>(tm_p1, tm_p0, tm_cf, shots, prog, L, shot_base, nshot, chunk, err, blockIdx.x,
-                                   blockIdx.y, blockIdx.z);
+                                   halves == 2 ? blockIdx.y : 2 * blockIdx.y, blockIdx.z);
 }
 
 // ------------------------------------------------------------ several groups in one launch

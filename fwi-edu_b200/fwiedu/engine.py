@@ -343,11 +343,13 @@ class Context:
         _check(self.L.fwi_ctx_set_allreduce(self.h, self._ar, None))
 
     def launch_shape(self):
-        """Shape of the last step launch (fwi_ctx_launch_shape, fwi_ctx_launch_variant)."""
-        v = [C.c_int() for _ in range(5)]
+        """Shape of the last step launch (fwi_ctx_launch_shape, fwi_ctx_launch_variant), and whether
+        the last pass ran as one persistent wavefront launch (fwi_ctx_launch_persistent)."""
+        v = [C.c_int() for _ in range(6)]
         _check(self.L.fwi_ctx_launch_shape(self.h, C.byref(v[0]), C.byref(v[1]), C.byref(v[2])))
         _check(self.L.fwi_ctx_launch_variant(self.h, C.byref(v[3]), C.byref(v[4])))
-        keys = ("tile_columns", "ring_depth", "shots_per_block", "groups_per_thread", "blocks_per_sm")
+        _check(self.L.fwi_ctx_launch_persistent(self.h, C.byref(v[5])))
+        keys = ("tile_columns", "ring_depth", "shots_per_block", "groups_per_thread", "blocks_per_sm", "persistent")
         return {k: x.value for k, x in zip(keys, v)}
 
     def stats(self):

@@ -217,6 +217,14 @@ FWI_API int fwi_ctx_launch_shape(fwi_ctx *ctx, int *tile_columns, int *ring_dept
  * the step kernel was compiled for (1: no minimum, coefficients in registers; 3: coefficients
  * read from shared memory).  No counterpart in the reference. */
 FWI_API int fwi_ctx_launch_variant(fwi_ctx *ctx, int *groups_per_thread, int *blocks_per_sm);
+/* 1 when the last pass ran as one persistent wavefront launch: on the batched path a forward pass
+ * (modeling, or the checkpointing forward of a gradient) whose 16-column tiles times shot ranges
+ * of at least two shots fit the GPU's resident blocks runs as a single cooperative launch in which
+ * every block owns one tile and shot range for all steps and waits only for its neighbouring
+ * tiles' previous step (FWI_WAVE=0 in the environment: step launches instead; same results bit
+ * for bit).  The shape functions then report that launch (tile width 16, its ring depth, shots
+ * per block, its resident blocks per SM).  No counterpart in the reference. */
+FWI_API int fwi_ctx_launch_persistent(fwi_ctx *ctx, int *persistent);
 
 /* CUDA graphs on the batched path (default on; FWI_GRAPH=0 in the environment turns them off):
  * off, every step is launched directly -- cheaper for a launch sequence run only once. */

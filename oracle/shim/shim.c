@@ -223,37 +223,47 @@ int fgettr(FILE *fp, segy *tp)
 int fvgettr(FILE *fp, segy *tp) { return fgettr(fp, tp); }
 
 /* ------------------------------------------------------------------- FFT */
-/* in-place complex FFT of length n, double precision; sign -1 forward, +1 backward */
-static void fft_pow2(double complex *a, int n, int sign)
+/* The transforms work in double precision and round to float at the plan's arrays.  Built with
+ * -DSHIM_FFT_FLOAT they work in float instead, as a single-precision FFT library does: the
+ * oracle uses that build to measure how much the reference's results depend on the rounding
+ * of the FFT library it is linked with. */
+#ifdef SHIM_FFT_FLOAT
+typedef float complex fftc_t;
+#else
+typedef double complex fftc_t;
+#endif
+
+/* in-place complex FFT of length n; sign -1 forward, +1 backward */
+static void fft_pow2(fftc_t *a, int n, int sign)
 {
     for (int i = 1, j = 0; i < n; i++) {
         int bit = n >> 1;
         for (; j & bit; bit >>= 1) j ^= bit;
         j ^= bit;
-        if (i < j) { double complex t = a[i]; a[i] = a[j]; a[j] = t; }
+        if (i < j) { fftc_t t = a[i]; a[i] = a[j]; a[j] = t; }
     }
     for (int len = 2; len <= n; len <<= 1) {
         double ang = sign * 2.0 * PI / len;
         for (int i = 0; i < n; i += len) {
             for (int k = 0; k < len / 2; k++) {
-                double complex w = cos(ang * k) + I * sin(ang * k);
-                double complex u = a[i + k], v = a[i + k + len / 2] * w;
+                fftc_t w = cos(ang * k) + I * sin(ang * k);
+                fftc_t u = a[i + k], v = a[i + k + len / 2] * w;
                 a[i + k] = u + v;
                 a[i + k + len / 2] = u - v;
             }
         }
     }
 }
-static void fft_any(double complex *a, int n, int sign)
+static void fft_any(fftc_t *a, int n, int sign)
 {
     if (n <= 1) return;
     if ((n & (n - 1)) == 0) { fft_pow2(a, n, sign); return; }
     /* Bluestein: chirp-z transform through a power-of-two convolution */
     int m = 1;
     while (m < 2 * n - 1) m <<= 1;
-    double complex *w = malloc(sizeof(double complex) * n);
-    double complex *A = calloc(m, sizeof(double complex));
-    double complex *B = calloc(m, sizeof(double complex));
+    fftc_t *w = malloc(sizeof(fftc_t) * n);
+    fftc_t *A = calloc(m, sizeof(fftc_t));
+    fftc_t *B = calloc(m, sizeof(fftc_t));
     for (int k = 0; k < n; k++) {
         /* k*k mod 2n keeps the chirp argument small */
         long long kk = ((long long)k * k) % (2LL * n);
@@ -301,9 +311,9 @@ void fftwf_plan_with_nthreads(int n) { (void)n; }
 void fftwf_cleanup_threads(void) {}
 
 /* full 2-D complex transform (row-major n0 x n1) */
-static void fft2(double complex *a, int n0, int n1, int sign)
+static void fft2(fftc_t *a, int n0, int n1, int sign)
 {
-    double complex *col = malloc(sizeof(double complex) * n0);
+    fftc_t *col = malloc(sizeof(fftc_t) * n0);
     for (int i = 0; i < n0; i++) fft_any(a + (size_t)i * n1, n1, sign);
     for (int j = 0; j < n1; j++) {
         for (int i = 0; i < n0; i++) col[i] = a[(size_t)i * n1 + j];
@@ -318,7 +328,7 @@ void fftwf_execute(const fftwf_plan p)
     int n = p->n0;
     if (p->kind == K_C2C) {
         float (*in)[2] = p->in, (*out)[2] = p->out;
-        double complex *a = malloc(sizeof(double complex) * (n ? n : 1));
+        fftc_t *a = malloc(sizeof(fftc_t) * (n ? n : 1));
         for (int i = 0; i < n; i++) a[i] = in[i][0] + I * in[i][1];
         fft_any(a, n, p->sign);
         for (int i = 0; i < n; i++) { out[i][0] = (float)creal(a[i]); out[i][1] = (float)cimag(a[i]); }
@@ -326,7 +336,7 @@ void fftwf_execute(const fftwf_plan p)
     } else if (p->kind == K_R2C) {
         float *in = p->in;
         float (*out)[2] = p->out;
-        double complex *a = malloc(sizeof(double complex) * (n ? n : 1));
+        fftc_t *a = malloc(sizeof(fftc_t) * (n ? n : 1));
         for (int i = 0; i < n; i++) a[i] = in[i];
         fft_any(a, n, -1);
         for (int i = 0; i <= n / 2; i++) { out[i][0] = (float)creal(a[i]); out[i][1] = (float)cimag(a[i]); }
@@ -334,7 +344,7 @@ void fftwf_execute(const fftwf_plan p)
     } else if (p->kind == K_C2R) {
         float (*in)[2] = p->in;
         float *out = p->out;
-        double complex *a = malloc(sizeof(double complex) * (n ? n : 1));
+        fftc_t *a = malloc(sizeof(fftc_t) * (n ? n : 1));
         for (int i = 0; i <= n / 2; i++) a[i] = in[i][0] + I * in[i][1];
         a[0] = creal(a[0]);
         if (n % 2 == 0) a[n / 2] = creal(a[n / 2]);
@@ -346,7 +356,7 @@ void fftwf_execute(const fftwf_plan p)
         int n0 = p->n0, n1 = p->n1, h = n1 / 2 + 1;
         float *in = p->in;
         float (*out)[2] = p->out;
-        double complex *a = malloc(sizeof(double complex) * (size_t)n0 * n1);
+        fftc_t *a = malloc(sizeof(fftc_t) * (size_t)n0 * n1);
         for (size_t i = 0; i < (size_t)n0 * n1; i++) a[i] = in[i];
         fft2(a, n0, n1, -1);
         for (int i = 0; i < n0; i++)
@@ -359,7 +369,7 @@ void fftwf_execute(const fftwf_plan p)
         int n0 = p->n0, n1 = p->n1, h = n1 / 2 + 1;
         float (*in)[2] = p->in;
         float *out = p->out;
-        double complex *a = malloc(sizeof(double complex) * (size_t)n0 * n1);
+        fftc_t *a = malloc(sizeof(fftc_t) * (size_t)n0 * n1);
         for (int i = 0; i < n0; i++)
             for (int j = 0; j < h; j++)
                 a[(size_t)i * n1 + j] = in[(size_t)i * h + j][0] + I * in[(size_t)i * h + j][1];

@@ -1,7 +1,8 @@
 """The TMA-fed step kernels in all of their launch shapes.
 
-The engine advances one step per launch by default (FWI_DEPTH=2 selects the two-step kernel,
-temporal blocking) and picks the tile width (8 or 16 columns, one-step
+Forward passes of two or more shots run by default as one persistent wavefront launch
+(fwi_wave.cuh; FWI_WAVE=0 turns it off, as these shape tests do); the step launches advance one
+step per launch by default (FWI_DEPTH=2 selects the two-step kernel, temporal blocking) and pick the tile width (8 or 16 columns, one-step
 kernel), the depth of the shared-memory stage ring (2 to 4 shots in flight) and the number of
 shots each block walks; environment variables override the choice.  Every shape must give the same bits: the reference's
 golden seismograms and gradient, and -- on a 12-shot survey where blocks walk more
@@ -41,7 +42,8 @@ SHAPES = [
     {"FWI_DEPTH": "1", "FWI_OCC": "3", "FWI_NST": "3", "FWI_CHUNK": "8"},
     {"FWI_DEPTH": "1", "FWI_OCC": "3", "FWI_NST": "2", "FWI_CHUNK": "1"},
 ]
-KEYS = ("FWI_TX", "FWI_NST", "FWI_CHUNK", "FWI_KERNEL", "FWI_MATH", "FWI_TUNE", "FWI_GPT", "FWI_OCC", "FWI_DEPTH")
+KEYS = ("FWI_TX", "FWI_NST", "FWI_CHUNK", "FWI_KERNEL", "FWI_MATH", "FWI_TUNE", "FWI_GPT", "FWI_OCC", "FWI_DEPTH",
+        "FWI_WAVE")
 
 
 def rel(a, b):
@@ -58,6 +60,9 @@ class env:
         self.old = {k: os.environ.get(k) for k in KEYS}
         for k in KEYS:
             os.environ.pop(k, None)
+        # the shapes are those of the step launches: forward passes too unless a case asks for
+        # the persistent wavefront launch
+        os.environ["FWI_WAVE"] = "0"
         os.environ.update(self.kv)
 
     def __exit__(self, *a):
@@ -188,3 +193,78 @@ def test_many_receivers_match_cp_async_kernel():
             got, _ = run_case(vp, rho, 10.0, 0.001, nt, 10, 1, shots)
         for i, (a, b) in enumerate(zip(got, ref)):
             assert np.array_equal(a, b), (shape, i)
+
+
+def run_persistent(vp, rho, dx, dt, nt, pml, fs, shots, obs=None):
+    """run_case with the wavefront launch on; also returns whether the pass used it"""
+    ctx = E.Context(0)
+    try:
+        ctx.set_model(vp, rho, dx, dx, dt, nt, pml, fs)
+        ctx.set_shots(shots)
+        if obs is None:
+            ctx.run(0, path=E.PATH_BATCHED)
+            return [ctx.traces(i) for i in range(len(shots))], None, ctx.launch_shape()["persistent"]
+        ctx.set_observed(obs)
+        ctx.run(1, 10.0, 2, 1, E.PATH_BATCHED)
+        return [ctx.traces(i) for i in range(len(shots))], ctx.gradient(), None
+    finally:
+        ctx.close()
+
+
+def test_wavefront_matches_golden():
+    """The persistent forward launch against the reference's golden seismograms and adjoint sources
+    (the two shots of the case whose windows span the model form one group; the third shot's
+    window differs), and its gradient -- whose checkpointing forward with the pseudo-Hessian runs
+    as the wavefront launch -- against the step launches', bit for bit."""
+    c = Case("fs1_small")
+    pick = [0, 2]
+    shots = [c.shots[i] for i in pick]
+    obs = [c.obs[i] for i in pick]
+    with env(FWI_WAVE="1"):
+        pre, _, used = run_persistent(c.vp, c.rho, c.dx, c.dt, c.nt, c.pml, c.fs, shots)
+        adj, grad, _ = run_persistent(c.vp0, c.rho0, c.dx, c.dt, c.nt, c.pml, c.fs, shots, obs=obs)
+    with env(FWI_WAVE="0"):
+        _, grad_ref = run_case(c.vp0, c.rho0, c.dx, c.dt, c.nt, c.pml, c.fs, shots, obs=obs)
+    assert used == 1
+    for k, i in enumerate(pick):
+        assert np.array_equal(pre[k], c.obs[i]), f"shot {i}"
+        assert np.array_equal(adj[k], c.adj[i]), f"adjoint source {i}"
+    assert np.array_equal(grad, grad_ref)
+
+
+@pytest.mark.parametrize("nshot", [2, 5, 12])
+def test_wavefront_matches_step_launches(nshot):
+    """Shot ranges of 2..n shots, several z-tiles and the receiver and source tiles: seismograms,
+    adjoint sources and gradient of the wavefront launch equal the step launches' bit for bit."""
+    vp, rho, shots, nt = survey12()
+    shots = shots[:nshot]
+    vp0 = M.smooth_model(vp, 8.0)
+    rho0 = M.gardner(vp0)
+    with env(FWI_WAVE="0"):
+        obs, _ = run_case(vp, rho, 10.0, 0.001, nt, 20, 1, shots)
+        adj_ref, grad_ref = run_case(vp0, rho0, 10.0, 0.001, nt, 20, 1, shots, obs=obs)
+    with env(FWI_WAVE="1"):
+        pre, _, used = run_persistent(vp, rho, 10.0, 0.001, nt, 20, 1, shots)
+        adj, grad, _ = run_persistent(vp0, rho0, 10.0, 0.001, nt, 20, 1, shots, obs=obs)
+    assert used == 1
+    assert all(np.array_equal(a, b) for a, b in zip(pre, obs))
+    assert all(np.array_equal(a, b) for a, b in zip(adj, adj_ref))
+    assert np.array_equal(grad, grad_ref)
+
+
+def test_wavefront_many_receivers():
+    """1500 receivers, one per column, on a shallow model: every sample taken inside the tiles
+    equals the step launches' sampling column, bit for bit."""
+    nz, nx, nt = 30, 1500, 120
+    vp = M.layered_model(nz, nx, seed=11, water_rows=4)
+    rho = M.gardner(vp, water_rows=4)
+    src = M.ricker(nt, 0.001, 15.0, 0.06)
+    sv = M.line_survey(nz, nx, 10.0, 10.0, 0.001, nt, 3, src, spacing_cells=400, first_cell=100)
+    shots = M.survey_shots(sv)
+    with env(FWI_WAVE="0"):
+        ref, _ = run_case(vp, rho, 10.0, 0.001, nt, 10, 1, shots)
+    with env(FWI_WAVE="1"):
+        got, _, used = run_persistent(vp, rho, 10.0, 0.001, nt, 10, 1, shots)
+    assert used == 1
+    for i, (a, b) in enumerate(zip(got, ref)):
+        assert np.array_equal(a, b), i
