@@ -145,7 +145,7 @@ struct fwi_ctx {
     bool use_graphs = true;  // capture the batched launch sequences as CUDA graphs
     bool pdl = true;         // consecutive steps as programmatic dependent launches
     bool tune = true;        // time the step kernel's launch shapes once per shape (autotune)
-    bool wave = true;        // forward passes as one persistent wavefront launch where they fit (FWI_WAVE)
+    bool wave = false;       // forward passes as one persistent wavefront launch where they fit (FWI_PERSIST=1)
     int *d_wave = nullptr;   // its abort word and per-block item counters
     int wave_cap = 0;
     std::map<std::string, long long> graph_launches;  // kernels each captured graph holds
@@ -262,7 +262,7 @@ extern "C" int fwi_ctx_create(fwi_ctx **out, int device, size_t budget)
     CK(cudaEventCreate(&c->ev1));
     TRY(dmalloc(c, (void **)&c->d_err, sizeof(int)));
     CK(cudaMemset(c->d_err, 0, sizeof(int)));
-    if (const char *e = getenv("FWI_WAVE")) c->wave = e[0] != '0';  // 0: forward passes as step launches
+    if (const char *e = getenv("FWI_PERSIST")) c->wave = e[0] != '0';  // 1: forward passes as one wavefront launch
     c->wave_cap = 4096;  // abort word + one counter per resident block (148 SMs x a few blocks)
     TRY(dmalloc(c, (void **)&c->d_wave, c->wave_cap * sizeof(int)));
     *out = c;

@@ -13,9 +13,9 @@
 // without a break.  The blocks are all resident (cooperative launch) and synchronise with
 // their eight neighbouring tiles only: item (L, s) may read the fields once the 3 x 3 tiles
 // around it have finished item (L-1, s) of the same shot range.  Each block publishes, in a
-// counter in global memory, how many of its items are complete; its producer warp publishes an
-// item as soon as the consumer warps have released its stage (their stores precede that
-// release), with a gpu-scope fence before the counter store, and acquires the neighbours'
+// counter in global memory, how many of its items are complete; its producer warp publishes
+// items once the consumer warps have released their stages (their stores precede that release),
+// in batches, with a gpu-scope fence before the counter store, and acquires the neighbours'
 // counters, followed by a proxy fence, before its tensor copies read what they wrote.  Every
 // dependency points at an earlier step, and publishing never waits for copies to be issued, so
 // the launch cannot deadlock while all blocks are resident.  The wavefront condition covers
@@ -30,13 +30,21 @@
 // Every wait is bounded: a counter or a copy that does not arrive within two seconds sets the
 // error word and the abort word; the other blocks see the abort word in their own waits, and
 // every block waits (bounded) for its copies in flight before it exits.
+//
+// Measured on B200 (60 shots, 221 x 601, 1001 steps): 57.8 us per step against 43.6 us for the
+// step launches, so the engine uses it only on request (FWI_PERSIST=1).  The fixed cost it removes
+// is real, but a block's tile is fixed for the whole pass: the tiles with the free surface and the
+// sources take the longer epilogue every step and pace every other tile through the dependency
+// chain (53.0 us with the receiver sampling removed, 48.0 us with every tile on the store-only
+// epilogue, both timing-only builds), while the step launches let the hardware balance uneven
+// blocks across the SMs.
 #pragma once
 #include "fwi_tile.cuh"
 
 namespace fwi {
 
 constexpr int WAVE_TX = 16;      // tile columns
-constexpr int WAVE_CH_MAX = 64;  // most shots one block owns
+constexpr int WAVE_CH_MAX = 32;  // most shots one block owns
 constexpr int WAVE_NB = 4;       // per-step scalar buffers: the consumers trail the producer by at
                                  // most ceil(NST / n) <= 2 steps (n >= 2 shots per block)
 
@@ -94,6 +102,9 @@ __global__ void __launch_bounds__(TG * WAVE_TX + 32, 3)
     __shared__ WaveShot s_shot[WAVE_NB][WAVE_CH_MAX];
     __shared__ int s_isx[WAVE_CH_MAX], s_isz[WAVE_CH_MAX], s_rz0[WAVE_CH_MAX], s_rz1[WAVE_CH_MAX];
     __shared__ double *s_H[WAVE_CH_MAX];
+    // receivers of the block's shots in its columns and rows: (trace << 8) | (row - first row of
+    // the tile) for the one receiver of a column; -1 none; -2 several (rare: read from the list)
+    __shared__ int s_rcv[WAVE_CH_MAX][WAVE_TX];
 
     const int b = blockIdx.x;
     const int tile = b / nranges, range = b - tile * nranges;
@@ -125,6 +136,22 @@ __global__ void __launch_bounds__(TG * WAVE_TX + 32, 3)
         s_rz1[tid] = D.rz1;
         s_H[tid] = D.H;
     }
+    if (tid < NC) {
+        const int z_a = 4 * G0, z_b = 4 * G0 + 4 * TG - 1;
+        for (int q = tid; q < nr * TX; q += NC) {
+            const int sq = q / TX, kq = q - sq * TX, xq = X0 + kq;
+            int code = -1;
+            if (xq < Nx) {
+                const ShotDesc &D = shots[cb + sq];
+                for (int e = D.colptr[xq]; e < D.colptr[xq + 1]; ++e) {
+                    const int2 r = D.rec[e];
+                    if (r.x < z_a || r.x > z_b) continue;
+                    code = code == -1 ? (r.y << 8) | (r.x - z_a) : -2;
+                }
+            }
+            s_rcv[sq][kq] = code;
+        }
+    }
     __syncthreads();
 
     if (warp == NW) {
@@ -136,24 +163,32 @@ __global__ void __launch_bounds__(TG * WAVE_TX + 32, 3)
             if (nx >= 0 && nx < ntx && nz >= 0 && nz < zt) nb = flags + 1 + (nz * ntx + nx) * nranges + range;
         }
         int seen = 0;        // the last value read from nb
-        int pub = 0;         // items published (lane 0's copy is the one that counts)
+        int done_l = 0;      // items whose stages the consumers have released (in order)
+        int pub = 0;         // items published in the counter (lane 0)
         bool failed = false;
         const u64 limit = 2000000000ull;
-        // warp-uniform: the wait begun at t0 has run out, or another block gave up
+        // warp-uniform: the wait begun at t0 has run out, or another block gave up (the abort word
+        // is read only once a wait has lasted 20 us: a normal wait is far shorter)
         auto expired = [&](u64 t0) {
-            return __any_sync(0xffffffffu, global_ns() - t0 > limit || *(volatile int *)abort_w != 0);
+            const u64 w = global_ns() - t0;
+            return __any_sync(0xffffffffu, w > limit || (w > 20000 && *(volatile int *)abort_w != 0));
         };
-        // publish the items whose stages the consumers have released, in order
-        auto publish = [&](int issued) {
+        // Count the items whose stages the consumers have released, and publish them: in batches
+        // of PUB_BATCH (each publication costs a gpu-scope fence, and the neighbours need an
+        // item only a step of the block's shots later), and all of them whenever the producer is
+        // about to wait for a neighbour or is done, so that no block ever waits on an item that
+        // its owner has finished but holds back.
+        constexpr int PUB_BATCH = 8;
+        auto publish = [&](int issued, bool force) {
             if (lane == 0) {
-                const int p0 = pub;
-                while (pub < issued && mbar_test(smem_u32(&empty[pub % NST]), (pub / NST) & 1)) ++pub;
-                if (pub != p0) {
+                while (done_l < issued && mbar_test(smem_u32(&empty[done_l % NST]), (done_l / NST) & 1)) ++done_l;
+                if (done_l != pub && (force || done_l - pub >= PUB_BATCH)) {
                     asm volatile("fence.acq_rel.gpu;" ::: "memory");
-                    st_relaxed(mine, pub);
+                    st_relaxed(mine, done_l);
+                    pub = done_l;
                 }
             }
-            pub = __shfl_sync(0xffffffffu, pub, 0);
+            done_l = __shfl_sync(0xffffffffu, done_l, 0);
         };
         if (lane == 0) {
             mbar_arrive_expect(smem_u32(&cfbar), Geo::CF_BYTES);
@@ -191,10 +226,12 @@ __global__ void __launch_bounds__(TG * WAVE_TX + 32, 3)
             const int st = j % NST;
             // the stage's previous item must be consumed (and is then published)
             if (j >= NST) {
+                // suspend on the stage's barrier (the hardware wakes the thread when it completes)
+                if (lane == 0 && done_l <= j - NST) mbar_try(smem_u32(&empty[st]), ((j - NST) / NST) & 1);
                 const u64 t0 = global_ns();
                 for (;;) {
-                    publish(j);
-                    if (pub > j - NST) break;
+                    publish(j, false);
+                    if (done_l > j - NST) break;
                     if (expired(t0)) {
                         failed = true;
                         break;
@@ -202,7 +239,8 @@ __global__ void __launch_bounds__(TG * WAVE_TX + 32, 3)
                 }
                 if (failed) break;
             }
-            // the neighbours' item (L-1, s)
+            // the neighbours' item (L-1, s); the counters seen last often cover it already
+            bool fresh = false;
             if (Lr > 0) {
                 const int need = (Lr - 1) * nr + s + 1;
                 const u64 t0 = global_ns();
@@ -211,19 +249,23 @@ __global__ void __launch_bounds__(TG * WAVE_TX + 32, 3)
                     if (!ok) {
                         seen = ld_acquire(nb);
                         ok = seen >= need;
+                        fresh = true;
                     }
                     if (__all_sync(0xffffffffu, ok)) break;
-                    publish(j);
+                    publish(j, true);
                     if (expired(t0)) {
                         failed = true;
                         break;
                     }
                 }
                 if (failed) break;
+                fresh = __any_sync(0xffffffffu, fresh);
             }
+            __syncwarp();  // the lanes' acquires precede lane 0's copies
             if (lane == 0) {
-                // the copies read what the neighbours stored: order them after the acquire
-                asm volatile("fence.proxy.async.global;" ::: "memory");
+                // the copies read what the neighbours stored: after a new acquire, order them
+                // behind it (copies after an earlier acquire are ordered by that one's fence)
+                if (fresh) asm volatile("fence.proxy.async.global;" ::: "memory");
                 const WaveStep &S = s_step[L & (WAVE_NB - 1)];
                 const unsigned bar = smem_u32(&full[st]);
                 mbar_arrive_expect(bar, Geo::P1_BYTES + Geo::P0_BYTES);
@@ -236,8 +278,9 @@ __global__ void __launch_bounds__(TG * WAVE_TX + 32, 3)
         // publish the rest as the consumers finish, then let the copies in flight land
         if (!failed) {
             const u64 t0 = global_ns();
-            while (pub < j) {
-                publish(j);
+            for (;;) {
+                publish(j, true);
+                if (done_l >= j) break;
                 if (expired(t0)) {
                     failed = true;
                     break;
@@ -319,9 +362,22 @@ __global__ void __launch_bounds__(TG * WAVE_TX + 32, 3)
         const unsigned wa = sb + (unsigned)((k + 3) * (TG + 2) + gl) * 16u;
         const float4 lo = lds4(wa), cq = lds4(wa + 16u), hi = lds4(wa + 32u);
         const int isx = s_isx[s], isz = s_isz[s];
-        const bool smp = S.sample && W.tr != nullptr && s_rz1[s] >= z_t0 && s_rz0[s] <= z_t1;
         const bool src_t = isx >= X0 && isx < X0 + TX && isz >= z_t0 && isz <= z_t1;
-        if (!(fs_tile || S.hess || smp || src_t)) {
+        // receivers sample u(t) before the step
+        if (S.sample && W.tr != nullptr && live) {
+            const int code = s_rcv[s][k];
+            if (code >= 0) {
+                const int row = z_t0 + (code & 255);
+                if (row >= z0 && row < z0 + 4) W.tr[code >> 8] = comp(cq, row - z0);
+            } else if (code == -2) {
+                const ShotDesc &D = shots[cb + s];
+                for (int e = __ldg(D.colptr + x), e1 = __ldg(D.colptr + x + 1); e < e1; ++e) {
+                    const int2 r = __ldg(D.rec + e);
+                    if (r.x >= z0 && r.x < z0 + 4) W.tr[r.y] = comp(cq, r.x - z0);
+                }
+            }
+        }
+        if (!(fs_tile || S.hess || src_t)) {
             // ---- store-only epilogue
             if (live) {
                 float4 p0;
@@ -329,15 +385,6 @@ __global__ void __launch_bounds__(TG * WAVE_TX + 32, 3)
                 *reinterpret_cast<float4 *>(W.out + colx + z0) = v;
             }
         } else if (live) {
-            // ---- receivers sample u(t) before the step
-            if (smp && z0 + 3 >= s_rz0[s] && z0 <= s_rz1[s]) {
-                const ShotDesc &D = shots[cb + s];
-                const int e0 = __ldg(D.colptr + x), e1 = __ldg(D.colptr + x + 1);
-                for (int e = e0; e < e1; ++e) {
-                    const int2 r = __ldg(D.rec + e);
-                    if (r.x >= z0 && r.x < z0 + 4) W.tr[r.y] = comp(cq, r.x - z0);
-                }
-            }
             // above the free surface (rows < pml): never updated, stored or accumulated
             if (!(A.fs && z0 + 3 < pml)) {
                 float4 p0;

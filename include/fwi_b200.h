@@ -217,13 +217,15 @@ FWI_API int fwi_ctx_launch_shape(fwi_ctx *ctx, int *tile_columns, int *ring_dept
  * the step kernel was compiled for (1: no minimum, coefficients in registers; 3: coefficients
  * read from shared memory).  No counterpart in the reference. */
 FWI_API int fwi_ctx_launch_variant(fwi_ctx *ctx, int *groups_per_thread, int *blocks_per_sm);
-/* 1 when the last pass ran as one persistent wavefront launch: on the batched path a forward pass
- * (modeling, or the checkpointing forward of a gradient) whose 16-column tiles times shot ranges
- * of at least two shots fit the GPU's resident blocks runs as a single cooperative launch in which
- * every block owns one tile and shot range for all steps and waits only for its neighbouring
- * tiles' previous step (FWI_WAVE=0 in the environment: step launches instead; same results bit
- * for bit).  The shape functions then report that launch (tile width 16, its ring depth, shots
- * per block, its resident blocks per SM).  No counterpart in the reference. */
+/* 1 when the last pass ran as one persistent wavefront launch.  With FWI_PERSIST=1 in the
+ * environment (default off), a forward pass on the batched path (modeling, or the checkpointing
+ * forward of a gradient) whose 16-column tiles times shot ranges of 2..32 shots fit the GPU's
+ * resident blocks runs as a single cooperative launch in which every block owns one tile and shot
+ * range for all steps and waits only for its neighbouring tiles' previous step; results are the
+ * step launches' bit for bit.  Off by default because it is slower on the benchmark survey (57.8
+ * against 43.6 us per step, 60 shots on 221 x 601): its tiles are assigned once, so the tiles with
+ * the free surface and the sources pace the whole grid, where the step launches' blocks balance
+ * them.  The shape functions then report that launch.  No counterpart in the reference. */
 FWI_API int fwi_ctx_launch_persistent(fwi_ctx *ctx, int *persistent);
 
 /* CUDA graphs on the batched path (default on; FWI_GRAPH=0 in the environment turns them off):

@@ -9,8 +9,13 @@ states the run and produced the expected outputs with the reference's own build)
 
 Compared with the reference's outputs: the modeling SU file byte for byte, the set of files
 each front-end writes (the engine's verbose files included), the misfit history, the first
-iteration's gradient and the final model within the FP32 tolerance of the FFT stages
-(1e-4 relative).
+iteration's gradient and the final model.  The tolerance of the last three is the reference's own
+precision for this run, stored with the expected outputs: how far they move when the reference is
+linked with a single-precision FFT instead of the double-precision one that made them
+(`fft_sensitivity`).  The 2 Hz stage filters the residual far below the wavelet's 10 Hz band, so
+its gradient moves by ~1.4e-4 relative under that change alone (the predicted data and the
+pseudo-Hessian stay bit-identical); the test allows three times each measured change, and never
+less than 1e-4 relative.
 """
 import hashlib
 import os
@@ -52,8 +57,10 @@ def test_demo_front_ends(tmp_path):
     def load(prefix):
         return np.fromfile(os.path.join(df, [f for f in files if f.startswith(prefix)][0]), np.float32)
 
+    sens_grad, sens_vp, sens_obj = (float(x) for x in want["fft_sensitivity"])
+    tol = lambda sens: max(1e-4, 3.0 * sens)  # noqa: E731
     obj = load("objective_function_")
     assert obj.shape == want["objective"].shape
-    assert np.all(np.abs(obj - want["objective"]) <= 1e-4 * np.abs(want["objective"]))
-    assert rel(load("grad_iter001_"), want["grad_iter001"]) <= 1e-4
-    assert rel(load("vp_inversion_"), want["vp_inversion"]) <= 1e-4
+    assert np.all(np.abs(obj - want["objective"]) <= tol(sens_obj) * np.abs(want["objective"]))
+    assert rel(load("grad_iter001_"), want["grad_iter001"]) <= tol(sens_grad)
+    assert rel(load("vp_inversion_"), want["vp_inversion"]) <= tol(sens_vp)

@@ -1,8 +1,8 @@
 """The TMA-fed step kernels in all of their launch shapes.
 
-Forward passes of two or more shots run by default as one persistent wavefront launch
-(fwi_wave.cuh; FWI_WAVE=0 turns it off, as these shape tests do); the step launches advance one
-step per launch by default (FWI_DEPTH=2 selects the two-step kernel, temporal blocking) and pick the tile width (8 or 16 columns, one-step
+Forward passes of two or more shots can run as one persistent wavefront launch (fwi_wave.cuh,
+FWI_PERSIST=1; off by default and in the shape tests); the step launches advance one step per
+launch by default (FWI_DEPTH=2 selects the two-step kernel, temporal blocking) and pick the tile width (8 or 16 columns, one-step
 kernel), the depth of the shared-memory stage ring (2 to 4 shots in flight) and the number of
 shots each block walks; environment variables override the choice.  Every shape must give the same bits: the reference's
 golden seismograms and gradient, and -- on a 12-shot survey where blocks walk more
@@ -43,7 +43,7 @@ SHAPES = [
     {"FWI_DEPTH": "1", "FWI_OCC": "3", "FWI_NST": "2", "FWI_CHUNK": "1"},
 ]
 KEYS = ("FWI_TX", "FWI_NST", "FWI_CHUNK", "FWI_KERNEL", "FWI_MATH", "FWI_TUNE", "FWI_GPT", "FWI_OCC", "FWI_DEPTH",
-        "FWI_WAVE")
+        "FWI_PERSIST")
 
 
 def rel(a, b):
@@ -62,7 +62,7 @@ class env:
             os.environ.pop(k, None)
         # the shapes are those of the step launches: forward passes too unless a case asks for
         # the persistent wavefront launch
-        os.environ["FWI_WAVE"] = "0"
+        os.environ["FWI_PERSIST"] = "0"
         os.environ.update(self.kv)
 
     def __exit__(self, *a):
@@ -220,10 +220,10 @@ def test_wavefront_matches_golden():
     pick = [0, 2]
     shots = [c.shots[i] for i in pick]
     obs = [c.obs[i] for i in pick]
-    with env(FWI_WAVE="1"):
+    with env(FWI_PERSIST="1"):
         pre, _, used = run_persistent(c.vp, c.rho, c.dx, c.dt, c.nt, c.pml, c.fs, shots)
         adj, grad, _ = run_persistent(c.vp0, c.rho0, c.dx, c.dt, c.nt, c.pml, c.fs, shots, obs=obs)
-    with env(FWI_WAVE="0"):
+    with env(FWI_PERSIST="0"):
         _, grad_ref = run_case(c.vp0, c.rho0, c.dx, c.dt, c.nt, c.pml, c.fs, shots, obs=obs)
     assert used == 1
     for k, i in enumerate(pick):
@@ -240,10 +240,10 @@ def test_wavefront_matches_step_launches(nshot):
     shots = shots[:nshot]
     vp0 = M.smooth_model(vp, 8.0)
     rho0 = M.gardner(vp0)
-    with env(FWI_WAVE="0"):
+    with env(FWI_PERSIST="0"):
         obs, _ = run_case(vp, rho, 10.0, 0.001, nt, 20, 1, shots)
         adj_ref, grad_ref = run_case(vp0, rho0, 10.0, 0.001, nt, 20, 1, shots, obs=obs)
-    with env(FWI_WAVE="1"):
+    with env(FWI_PERSIST="1"):
         pre, _, used = run_persistent(vp, rho, 10.0, 0.001, nt, 20, 1, shots)
         adj, grad, _ = run_persistent(vp0, rho0, 10.0, 0.001, nt, 20, 1, shots, obs=obs)
     assert used == 1
@@ -261,9 +261,9 @@ def test_wavefront_many_receivers():
     src = M.ricker(nt, 0.001, 15.0, 0.06)
     sv = M.line_survey(nz, nx, 10.0, 10.0, 0.001, nt, 3, src, spacing_cells=400, first_cell=100)
     shots = M.survey_shots(sv)
-    with env(FWI_WAVE="0"):
+    with env(FWI_PERSIST="0"):
         ref, _ = run_case(vp, rho, 10.0, 0.001, nt, 10, 1, shots)
-    with env(FWI_WAVE="1"):
+    with env(FWI_PERSIST="1"):
         got, _, used = run_persistent(vp, rho, 10.0, 0.001, nt, 10, 1, shots)
     assert used == 1
     for i, (a, b) in enumerate(zip(got, ref)):
