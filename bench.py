@@ -632,6 +632,37 @@ def fp64_error(E, vp, rho, vp0, rho0, shots, local=0):
                       "FP32 observed data", "tolerances": {"seismogram": 1e-5, "gradient": 1e-4}}
 
 
+def contracted_arithmetic(E, local, vp, rho, vp0, rho0, shots, obs, peaks, steps=2):
+    """The same iteration with the contracted arithmetic (FWI_MATH=1: multiply-adds fused into
+    packed FMAs; within the stated FP32 tolerances, not bit-identical to the reference): its
+    throughput, the forward step kernel's roofline, and its error against the FP64 build."""
+    old = os.environ.get("FWI_MATH")
+    os.environ["FWI_MATH"] = "1"
+    try:
+        ctx = E.Context(local)
+        try:
+            ctx.set_model(vp, rho, DX, DX, DT, NT, PML, FS)
+            ctx.set_shots(shots)
+            roof = step_roofline(ctx, E, peaks)
+            ctx.set_model(vp0, rho0, DX, DX, DT, NT, PML, FS)
+            ctx.set_observed(obs)
+            params = E.IterParams(path=E.PATH_BATCHED, **ITER)
+            ctx.fwi_iteration(params)
+            ms = [ctx.fwi_iteration(params)["ms"] for _ in range(steps)]
+        finally:
+            ctx.close()
+        err = fp64_error(E, vp, rho, vp0, rho0, shots, local)
+    finally:
+        if old is None:
+            os.environ.pop("FWI_MATH", None)
+        else:
+            os.environ["FWI_MATH"] = old
+    return {"value": NSHOT * steps / (sum(ms) / 1e3), "unit": UNIT, "ms_per_step": sum(ms) / steps,
+            "roofline_frac": roof["frac"], "launch_us": roof["launch_us"], "fp64_error": err,
+            "note": "FWI_MATH=1, device-timed like value after one warm-up iteration; the headline value "
+                    "keeps the reference's separately rounded products (bit-identical results)"}
+
+
 def step_case(nshot, nt):
     """A short batched forward on the survey model (the step kernel's launch shape at full size)
     for profilers: `ncu ... python bench.py --step-case 60 40`."""
@@ -826,6 +857,13 @@ def main():
         except Exception as ex:  # a reported statement, never required
             err64 = {"unavailable": str(ex)}
 
+    contracted = None
+    if rank == 0 and world == 1 and not args.no_extra and not args.no_cpu:
+        try:
+            contracted = contracted_arithmetic(E, local, vp, rho, vp0, rho0, shots, obs, peaks)
+        except Exception as ex:  # a reported comparison, never required
+            contracted = {"unavailable": str(ex)}
+
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
         try:
@@ -858,7 +896,7 @@ def main():
                                             "occupancy and shared coefficient reads, not an order of magnitude"),
                 "uneven_batch": uneven, "large_survey": large,
                 "wall_s": wall, "gpu_launches": launches, "roofline": roof, "roofline_adjoint": roof_adj,
-                "fp64_error": err64, "cpu_baseline": cpu, "e2e": e2e,
+                "fp64_error": err64, "contracted_arithmetic": contracted, "cpu_baseline": cpu, "e2e": e2e,
                 "serving": serve,
                 "clocks": clk.summary()}
         print(json.dumps(line), flush=True)
