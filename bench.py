@@ -555,13 +555,23 @@ def step_roofline(ctx, E, peaks):
     bytes_per_launch = cells_per_launch * bpc
     achieved = bytes_per_launch / (per_launch_ms * 1e-3) / 1e9
     peak = peaks.get("hbm_gbs")
-    traffic = tinfo = None
+    traffic = tinfo = rw = None
     if os.path.exists(TRAFFIC):
         tinfo = json.load(open(TRAFFIC))
-        traffic = tinfo["dram_read_bytes"] + tinfo["dram_write_bytes"]
+        # the steady-state capture (L2 carried over between launches, so that the write-backs a
+        # launch leaves in L2 are counted in the launches that evict them) where there is one
+        src = tinfo.get("steady_state", tinfo)
+        traffic = src["dram_read_bytes"] + src["dram_write_bytes"]
+        alg_read = cells_per_launch * (8.0 + 24.0 / S)
+        alg_write = cells_per_launch * 4.0
+        rw = {"read_bytes": src["dram_read_bytes"], "write_bytes": src["dram_write_bytes"],
+              "read_vs_algorithmic": src["dram_read_bytes"] / alg_read,
+              "write_vs_algorithmic": src["dram_write_bytes"] / alg_write,
+              "capture": src.get("cache_control", "all")}
     return {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
             "frac": achieved / peak if peak else None, "traffic": traffic,
             "traffic_vs_algorithmic": traffic / bytes_per_launch if traffic else None,
+            "traffic_read_write": rw,
             "traffic_source": tinfo.get("kernel") if tinfo else None,
             "kernel": "step kernel (batched forward, 60 shots per launch)",
             "steps_per_launch": steps_per_launch,

@@ -59,6 +59,44 @@ __device__ __forceinline__ T cmulc(T a, T b)
     return r;
 }
 
+// The core of an M-point circular convolution of the P sequences in fbuf (each loaded at its
+// bit-reversed positions): radix-2 decimation in time (natural order out), multiplication by the
+// spectrum G (which carries the 1 / M), and the inverse by decimation in frequency with conjugate
+// twiddles (bit-reversed order out).  Every thread of the block takes part.
+template <class R>
+__device__ __forceinline__ void fft_conv_core(typename Cplx<R>::T *fbuf, int P, int M, int logM,
+                                              const typename Cplx<R>::T *G, const typename Cplx<R>::T *tw)
+{
+    typedef typename Cplx<R>::T C;
+    const int tid = threadIdx.x, nth = blockDim.x, half_M = M >> 1;
+    for (int len = 2, lg = 1; len <= M; len <<= 1, ++lg) {
+        const int half = len >> 1, tstep = M >> lg;
+        for (int b = tid; b < P * half_M; b += nth) {
+            const int q = b / half_M, bb = b - q * half_M;
+            const int p = bb & (half - 1), i = ((bb >> (lg - 1)) << lg) + p, j = i + half;
+            C *f = fbuf + q * M;
+            const C t = cmulc(tw[p * tstep], f[j]), a = f[i];
+            f[i] = Cplx<R>::make(a.x + t.x, a.y + t.y);
+            f[j] = Cplx<R>::make(a.x - t.x, a.y - t.y);
+        }
+        __syncthreads();
+    }
+    for (int i = tid; i < P * M; i += nth) fbuf[i] = cmulc(fbuf[i], G[i & (M - 1)]);
+    __syncthreads();
+    for (int len = M, lg = logM; len >= 2; len >>= 1, --lg) {
+        const int half = len >> 1, tstep = M >> lg;
+        for (int b = tid; b < P * half_M; b += nth) {
+            const int q = b / half_M, bb = b - q * half_M;
+            const int p = bb & (half - 1), i = ((bb >> (lg - 1)) << lg) + p, j = i + half;
+            C *f = fbuf + q * M;
+            const C w = tw[p * tstep], a = f[i], c = f[j];
+            f[i] = Cplx<R>::make(a.x + c.x, a.y + c.y);
+            f[j] = cmulc(Cplx<R>::make(a.x - c.x, a.y - c.y), Cplx<R>::make(w.x, -w.y));
+        }
+        __syncthreads();
+    }
+}
+
 // grid: ceil(nseq / (2 P)) blocks; dynamic shared memory P * M complex values of type R
 template <class R>
 static __global__ void __launch_bounds__(512) k_fft_conv(const ConvDesc d)
@@ -67,7 +105,7 @@ static __global__ void __launch_bounds__(512) k_fft_conv(const ConvDesc d)
     extern __shared__ __align__(16) unsigned char fsm[];
     C *fbuf = reinterpret_cast<C *>(fsm);
     const C *G = static_cast<const C *>(d.G), *tw = static_cast<const C *>(d.tw);
-    const int M = d.M, P = d.P, half_M = M >> 1;
+    const int M = d.M, P = d.P;
     const int s0 = blockIdx.x * 2 * P;  // first sequence of the block
     const int tid = threadIdx.x, nth = blockDim.x;
     for (int i = tid; i < P * M; i += nth) fbuf[i] = Cplx<R>::make(0, 0);
@@ -84,34 +122,7 @@ static __global__ void __launch_bounds__(512) k_fft_conv(const ConvDesc d)
         c[sl & 1] = (R)v;
     }
     __syncthreads();
-    // forward: decimation in time, bit-reversed in, natural order out
-    for (int len = 2, lg = 1; len <= M; len <<= 1, ++lg) {
-        const int half = len >> 1, tstep = M >> lg;
-        for (int b = tid; b < P * half_M; b += nth) {
-            const int q = b / half_M, bb = b - q * half_M;
-            const int p = bb & (half - 1), i = ((bb >> (lg - 1)) << lg) + p, j = i + half;
-            C *f = fbuf + q * M;
-            const C t = cmulc(tw[p * tstep], f[j]), a = f[i];
-            f[i] = Cplx<R>::make(a.x + t.x, a.y + t.y);
-            f[j] = Cplx<R>::make(a.x - t.x, a.y - t.y);
-        }
-        __syncthreads();
-    }
-    for (int i = tid; i < P * M; i += nth) fbuf[i] = cmulc(fbuf[i], G[i & (M - 1)]);
-    __syncthreads();
-    // inverse: decimation in frequency with conjugate twiddles, natural in, bit-reversed out
-    for (int len = M, lg = d.logM; len >= 2; len >>= 1, --lg) {
-        const int half = len >> 1, tstep = M >> lg;
-        for (int b = tid; b < P * half_M; b += nth) {
-            const int q = b / half_M, bb = b - q * half_M;
-            const int p = bb & (half - 1), i = ((bb >> (lg - 1)) << lg) + p, j = i + half;
-            C *f = fbuf + q * M;
-            const C w = tw[p * tstep], a = f[i], c = f[j];
-            f[i] = Cplx<R>::make(a.x + c.x, a.y + c.y);
-            f[j] = cmulc(Cplx<R>::make(a.x - c.x, a.y - c.y), Cplx<R>::make(w.x, -w.y));
-        }
-        __syncthreads();
-    }
+    fft_conv_core<R>(fbuf, P, M, d.logM, G, tw);
     for (int t = tid; t < d.n_out * nsb; t += nth) {
         const int i = t / nsb, sl = t % nsb;
         float v = 0.f;
@@ -121,6 +132,86 @@ static __global__ void __launch_bounds__(512) k_fft_conv(const ConvDesc d)
             v = (float)c[sl & 1];
         }
         d.out[(long long)(s0 + sl) * d.out_ss + (long long)i * d.out_es] = v;
+    }
+}
+
+// ---------------------------------------------------------------- DFTs of any length (Bluestein)
+// An N-point DFT X_k = sum_j x_j e^{-2 pi i jk / N} is conj(b_k) times the convolution of
+// u_j = x_j conj(b_j) with b, b_m = e^{i pi m^2 / N} (jk = (j^2 + k^2 - (k - j)^2) / 2); the inverse
+// direction (e^{+2 pi i jk / N}) uses the conjugate chirps.  The convolution runs as the M-point
+// one above (M the power of two >= 2N - 1) with the spectrum of b wrapped onto M points.
+// With a window, the first DFT's result is multiplied by a real window and transformed again in
+// the opposite direction in the same block: the chirp that ends the first DFT and the one that
+// starts the second multiply to |b_j|^2 = 1, so the window multiplies the convolution's output.
+struct BlueDesc {
+    const void *in;             // input: element j of sequence s at in[s * in_ss + j * in_es]
+    long long in_es, in_ss;
+    int in_cplx;                // 1: float2 values, 0: float (imaginary part 0)
+    void *out;                  // output position k (o0 <= k < o0 + no) of sequence s at
+    long long out_es, out_ss;   //   out[s * out_ss + (k - o0) * out_es]
+    int out_real;               // 1: the real part as float, divided by `divisor`; 0: float2
+    float divisor;
+    int o0, no;
+    int N, nseq, M, logM, P;
+    int dir;                    // direction of the first DFT: -1 forward, +1 inverse
+    const float *win;           // null, or the window: position k of sequence s at win[k * win_es + s * win_ss]
+    long long win_es, win_ss;
+    const void *tables;         // fwi_bluestein_tables: chirp (N), spectrum of b (M), of conj(b) (M)
+    const void *tw;             // exp(-2 pi i k / M), k < M / 2
+    int dbl;                    // tables and transforms in FP64
+};
+
+// grid: ceil(nseq / P) blocks; dynamic shared memory P * M complex values of type R
+template <class R>
+static __global__ void __launch_bounds__(512) k_bluestein(const BlueDesc d)
+{
+    typedef typename Cplx<R>::T C;
+    extern __shared__ __align__(16) unsigned char fsm[];
+    C *fbuf = reinterpret_cast<C *>(fsm);
+    const C *chirp = static_cast<const C *>(d.tables), *Bf = chirp + d.N, *Bi = Bf + d.M;
+    const C *tw = static_cast<const C *>(d.tw);
+    const int M = d.M, P = d.P, N = d.N, sh = 32 - d.logM;
+    const int s0 = blockIdx.x * P, nsb = min(P, d.nseq - s0);
+    const int tid = threadIdx.x, nth = blockDim.x;
+    for (int i = tid; i < P * M; i += nth) fbuf[i] = Cplx<R>::make(0, 0);
+    __syncthreads();
+    for (int t = tid; t < N * nsb; t += nth) {
+        const int j = t / nsb, sl = t - j * nsb;
+        const long long a = (long long)(s0 + sl) * d.in_ss + (long long)j * d.in_es;
+        C v;
+        if (d.in_cplx) {
+            const float2 f = static_cast<const float2 *>(d.in)[a];
+            v = Cplx<R>::make(f.x, f.y);
+        } else {
+            v = Cplx<R>::make(static_cast<const float *>(d.in)[a], 0);
+        }
+        const C b = chirp[j];
+        fbuf[sl * M + (__brev((unsigned)j) >> sh)] = cmulc(v, Cplx<R>::make(b.x, d.dir < 0 ? -b.y : b.y));
+    }
+    __syncthreads();
+    fft_conv_core<R>(fbuf, P, M, d.logM, d.dir < 0 ? Bf : Bi, tw);
+    int dir = d.dir;
+    if (d.win) {
+        for (int i = tid; i < P * M; i += nth) {
+            const int sl = i / M, p = i - sl * M, j = (int)(__brev((unsigned)p) >> sh);
+            if (sl < nsb && j < N) {
+                const R w = (R)d.win[(long long)j * d.win_es + (long long)(s0 + sl) * d.win_ss];
+                fbuf[i] = Cplx<R>::make(fbuf[i].x * w, fbuf[i].y * w);
+            } else {
+                fbuf[i] = Cplx<R>::make(0, 0);
+            }
+        }
+        __syncthreads();
+        dir = -dir;
+        fft_conv_core<R>(fbuf, P, M, d.logM, dir < 0 ? Bf : Bi, tw);
+    }
+    for (int t = tid; t < d.no * nsb; t += nth) {
+        const int kk = t / nsb, sl = t - kk * nsb, k = d.o0 + kk;
+        const C b = chirp[k];
+        const C v = cmulc(fbuf[sl * M + (__brev((unsigned)k) >> sh)], Cplx<R>::make(b.x, dir < 0 ? -b.y : b.y));
+        const long long a = (long long)(s0 + sl) * d.out_ss + (long long)kk * d.out_es;
+        if (d.out_real) static_cast<float *>(d.out)[a] = (float)v.x / d.divisor;
+        else static_cast<float2 *>(d.out)[a] = make_float2((float)v.x, (float)v.y);
     }
 }
 
@@ -153,6 +244,31 @@ static inline cudaError_t launch_fft_conv(ConvDesc d, cudaStream_t st)
     const int blocks = (d.nseq + 2 * d.P - 1) / (2 * d.P);
     if (d.dbl) k_fft_conv<double><<<blocks, 512, smem, st>>>(d);
     else k_fft_conv<float><<<blocks, 512, smem, st>>>(d);
+    return cudaGetLastError();
+}
+
+// fills M, logM and P of d (M = the power of two >= 2N - 1, for which the tables were built) and
+// launches; cudaErrorInvalidValue when M > FFT_CONV_MAX, the output range leaves [0, N), or d.dbl
+// does not match conv_in_f64(M)
+static inline cudaError_t launch_bluestein(BlueDesc d, cudaStream_t st)
+{
+    int M = 2, lg = 1;
+    while (M < 2 * d.N - 1) M <<= 1, ++lg;
+    if (M > FFT_CONV_MAX || d.N < 1 || d.nseq < 1 || d.o0 < 0 || d.no < 1 || d.o0 + d.no > d.N ||
+        (d.dbl != 0) != conv_in_f64(M))
+        return cudaErrorInvalidValue;
+    d.M = M;
+    d.logM = lg;
+    const size_t csize = d.dbl ? 16 : 8;
+    d.P = M >= 8192 ? 1 : 8192 / M;
+    d.P = d.P < d.nseq ? d.P : d.nseq;
+    const size_t smem = (size_t)d.P * M * csize;
+    const void *fn = d.dbl ? (const void *)k_bluestein<double> : (const void *)k_bluestein<float>;
+    cudaError_t e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return e;
+    const int blocks = (d.nseq + d.P - 1) / d.P;
+    if (d.dbl) k_bluestein<double><<<blocks, 512, smem, st>>>(d);
+    else k_bluestein<float><<<blocks, 512, smem, st>>>(d);
     return cudaGetLastError();
 }
 

@@ -3,7 +3,6 @@
 // front-end written against FWI-EDU links unchanged; each call stages its arrays
 // through one process-wide device workspace.  The device-resident FWI iteration of
 // fwi_engine.cu runs the same kernels without the host round trips.
-#include <cublas_v2.h>
 #include <cuda_runtime.h>
 
 #include <cmath>
@@ -69,21 +68,8 @@ bool ops_ready(size_t bytes)
 
 size_t al(size_t b) { return (b + 255) & ~size_t(255); }
 
-// ---- operator matrices of the 2-D wavenumber filters, applied by FP32 GEMM
-cublasHandle_t g_blas = nullptr;
-std::map<std::string, float *> g_opmats;  // built once per (kind, size, parameters) and kept
-
-bool blas_ready()
-{
-    if (!g_blas) {
-        if (cublasCreate(&g_blas) != CUBLAS_STATUS_SUCCESS) {
-            fprintf(stderr, "<error>: cublasCreate failed\n");
-            return false;
-        }
-        cublasSetMathMode(g_blas, CUBLAS_PEDANTIC_MATH);  // plain FP32, no TF32
-    }
-    return cublasSetStream(g_blas, g_ops.st) == CUBLAS_STATUS_SUCCESS;
-}
+// ---- device tables built once on the host per (kind, size, parameters) and kept
+std::map<std::string, float *> g_opmats;
 
 std::string fbits(float v)
 {
@@ -418,19 +404,51 @@ void build_wn_window(float *h, const int *ip, const float *fp)
 {
     fwi_wavenumber_window(ip[0], ip[1], ip[2], fp[0], fp[1], fp[2], fp[3], h);
 }
-void build_wn_fz(float *h, const int *ip, const float *) { fwi_wn_forward_z(ip[0], ip[1], h); }
-void build_wn_fx(float *h, const int *ip, const float *) { fwi_wn_forward_x(ip[0], ip[1], h); }
-void build_wn_ix(float *h, const int *ip, const float *) { fwi_wn_inverse_x(ip[0], ip[1], h); }
-void build_wn_iz(float *h, const int *ip, const float *) { fwi_wn_inverse_z(ip[0], ip[1], h); }
-
-// F[c][r] *= W[c mod Nx][r] over the two Nz x Nx halves (real, imaginary) of the spectrum
-__global__ void k_window2(float *__restrict__ F, const float *__restrict__ W, long long plane)
+void build_bluestein(float *h, const int *ip, const float *)
 {
-    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < 2 * plane;
-         i += (long long)gridDim.x * blockDim.x)
-        F[i] *= W[i < plane ? i : i - plane];
+    fwi_bluestein_tables(ip[0], fwi_conv_size(ip[0]), conv_in_f64(fwi_conv_size(ip[0])) ? 1 : 0, h);
 }
 
+// the chirp and spectra of an N-point DFT, and the twiddles of its convolution size, into d
+bool dft_tables(int N, BlueDesc *d)
+{
+    const int M = fwi_conv_size(N);
+    if (M > FFT_CONV_MAX) {
+        fprintf(stderr, "<error>: a DFT of length %d needs %d-point transforms (at most %d)\n", N, M, FFT_CONV_MAX);
+        return false;
+    }
+    const bool f64 = conv_in_f64(M);
+    const int ip[1] = {N}, ipt[1] = {M};
+    const float *t = op_matrix("bl/" + std::to_string(N), (size_t)(f64 ? 2 : 1) * 2 * (N + 2 * (size_t)M),
+                               build_bluestein, ip, nullptr);
+    const float *tw = op_matrix("tw/" + std::to_string(M), (size_t)(f64 ? 2 : 1) * M, build_twiddles, ipt, nullptr);
+    if (!t || !tw) return false;
+    d->tables = t;
+    d->tw = tw;
+    d->dbl = f64 ? 1 : 0;
+    d->N = N;
+    return true;
+}
+
+// the edge-replicating pad of pad_model2d (common.c:110-170): padded sample (z, x) takes the
+// model's sample at the clamped position
+__global__ void k_pad_replicate(const float *__restrict__ x, int nz, int nx, int pad, float *__restrict__ y, int Nz,
+                                long long plane)
+{
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < plane;
+         i += (long long)gridDim.x * blockDim.x) {
+        const int X = (int)(i / Nz), Z = (int)(i - (long long)X * Nz);
+        const int xs = min(max(X - pad, 0), nx - 1), zs = min(max(Z - pad, 0), nz - 1);
+        y[i] = x[(long long)xs * nz + zs];
+    }
+}
+
+// lowpass2d / bandpass2d: taper, edge-replicating pad, 2-D DFT of the padded field, the
+// reference's float window, inverse 2-D DFT, / (Nz Nx), crop (common.c:1042-1284).  The DFTs have
+// the padded field's own sizes (the window is defined on that grid) and run as Bluestein
+// transforms on the device in three launches: the z transforms of every padded column; for every
+// z wavenumber the x transform, the window and the inverse x transform, kept at the model's
+// columns only; the inverse z transforms of those columns, kept at the model's rows.
 void wavenumber_filter(float **s, int nz, int nx, float dz, float dx, float kpass, float kcut, float **s_filter,
                        int filter, const char *name)
 {
@@ -452,63 +470,58 @@ void wavenumber_filter(float **s, int nz, int nx, float dz, float dx, float kpas
         fprintf(stderr, "<error>: %s: padded field %lld x %lld too large\n", name, Nz, Nx);
         return;
     }
+    BlueDesc dz_{}, dx_{};
+    if (!dft_tables((int)Nz, &dz_) || !dft_tables((int)Nx, &dx_)) return;
     std::vector<float> tct(Lt + 1), tcr(Lr + 1);
     if (Lt > 0) fwi_taper_coefs(Lt, tct.data());
     if (Lr > 0) fwi_taper_coefs(Lr, tcr.data());
     const size_t m = (size_t)nz * nx, plane = (size_t)(Nz * Nx);
-    const size_t bx = al(m * 4), bT = al((size_t)Nz * 2 * nx * 4), bF = al(2 * plane * 4), bV = bT;
+    const size_t bx = al(m * 4), bP = al(plane * 4), bA = al(plane * 8), bG = al((size_t)nx * Nz * 8);
     const size_t bt = al((Lt + 1) * 4) + al((Lr + 1) * 4);
-    if (!ops_ready(2 * bx + bT + bF + bV + bt + al(sizeof(TaperDesc)) + 256) || !blas_ready()) return;
+    if (!ops_ready(2 * bx + bP + bA + bG + bt + al(sizeof(TaperDesc)) + 256)) return;
     char *b = g_ops.buf;
-    float *x = (float *)b, *T = (float *)(b + bx), *F = (float *)(b + bx + bT), *V = (float *)(b + bx + bT + bF);
-    float *Y = (float *)(b + bx + bT + bF + bV);
-    float *dct = (float *)(b + 2 * bx + bT + bF + bV), *dcr = (float *)((char *)dct + al((Lt + 1) * 4));
-    TaperDesc *td = (TaperDesc *)(b + 2 * bx + bT + bF + bV + bt);
+    float *x = (float *)b, *P = (float *)(b + bx);
+    float2 *A = (float2 *)(b + bx + bP), *Gc = (float2 *)(b + bx + bP + bA);
+    float *Y = (float *)(b + bx + bP + bA + bG);
+    float *dct = (float *)(b + 2 * bx + bP + bA + bG), *dcr = (float *)((char *)dct + al((Lt + 1) * 4));
+    TaperDesc *td = (TaperDesc *)(b + 2 * bx + bP + bA + bG + bt);
 
     const int iNx = (int)Nx, iNz = (int)Nz;
-    const int wi[3] = {filter, iNx, iNz}, zi[2] = {nz, pad}, xi[2] = {nx, pad};
+    const int wi[3] = {filter, iNx, iNz};
     const float wf[4] = {dx, dz, kpass, kcut};
-    const std::string sz = "/" + std::to_string(nz) + "/" + std::to_string(pad), sx = "/" + std::to_string(nx) + "/" +
-                                                                                    std::to_string(pad);
-    const float *Wd = op_matrix("w2/" + std::to_string(filter) + "/" + std::to_string(iNx) + "/" +
-                                    std::to_string(iNz) + "/" + fbits(dx) + "/" + fbits(dz) + "/" + fbits(kpass) +
-                                    "/" + fbits(kcut),
-                                plane, build_wn_window, wi, wf);
-    const float *Az = op_matrix("wfz" + sz, 2 * (size_t)Nz * nz, build_wn_fz, zi, nullptr);
-    const float *Rf = op_matrix("wfx" + sx, 4 * (size_t)Nx * nx, build_wn_fx, xi, nullptr);
-    const float *Ri = op_matrix("wix" + sx, 4 * (size_t)Nx * nx, build_wn_ix, xi, nullptr);
-    const float *Lz_ = op_matrix("wiz" + sz, 2 * (size_t)Nz * nz, build_wn_iz, zi, nullptr);
-    if (!Wd || !Az || !Rf || !Ri || !Lz_) return;
+    const float *W = op_matrix("w2/" + std::to_string(filter) + "/" + std::to_string(iNx) + "/" +
+                                   std::to_string(iNz) + "/" + fbits(dx) + "/" + fbits(dz) + "/" + fbits(kpass) +
+                                   "/" + fbits(kcut),
+                               plane, build_wn_window, wi, wf);
+    if (!W) return;
 
     cudaMemcpyAsync(x, s[0], m * 4, cudaMemcpyHostToDevice, g_ops.st);
     cudaMemcpyAsync(dct, tct.data(), (Lt + 1) * 4, cudaMemcpyHostToDevice, g_ops.st);
     cudaMemcpyAsync(dcr, tcr.data(), (Lr + 1) * 4, cudaMemcpyHostToDevice, g_ops.st);
     if (!taper_device(x, nz, nx, Lt, Lr, dct, dcr, td)) return;
     cudaMemcpyAsync(s[0], x, m * 4, cudaMemcpyDeviceToHost, g_ops.st);  // the reference tapers its input
-
-    const float one = 1.0f, zero = 0.0f, inv = 1.0f / (float)(Nz * Nx);
-    bool ok =
-        // [Tr | Ti] = [C'z X | -S'z X]                                         (Nz x 2nx)
-        cublasSgemmStridedBatched(g_blas, CUBLAS_OP_N, CUBLAS_OP_N, iNz, nx, nz, &one, Az, iNz, (long long)Nz * nz, x,
-                                  nz, 0, &zero, T, iNz, (long long)Nz * nx, 2) == CUBLAS_STATUS_SUCCESS &&
-        // [Fr | Fi] = [Tr | Ti] [[C'x^T, -S'x^T], [S'x^T, C'x^T]]               (Nz x 2Nx)
-        cublasSgemm(g_blas, CUBLAS_OP_N, CUBLAS_OP_N, iNz, 2 * iNx, 2 * nx, &one, T, iNz, Rf, 2 * nx, &zero, F, iNz) ==
-            CUBLAS_STATUS_SUCCESS;
-    if (ok) {
-        k_window2<<<592, 256, 0, g_ops.st>>>(F, Wd, (long long)plane);
-        ok = report(cudaGetLastError(), "k_window2");
-    }
-    ok = ok &&
-         // Vr, Vi = [Gr | Gi] times the two column blocks of the inverse x operator, stacked (2Nz x nx)
-         cublasSgemm(g_blas, CUBLAS_OP_N, CUBLAS_OP_N, iNz, nx, 2 * iNx, &one, F, iNz, Ri, 2 * iNx, &zero, V,
-                     2 * iNz) == CUBLAS_STATUS_SUCCESS &&
-         cublasSgemm(g_blas, CUBLAS_OP_N, CUBLAS_OP_N, iNz, nx, 2 * iNx, &one, F, iNz, Ri + 2 * Nx * nx, 2 * iNx,
-                     &zero, V + Nz, 2 * iNz) == CUBLAS_STATUS_SUCCESS &&
-         // Y = [Cz | -Sz] [Vr; Vi] / (Nz Nx) at the kept rows                    (nz x nx)
-         cublasSgemm(g_blas, CUBLAS_OP_N, CUBLAS_OP_N, nz, nx, 2 * iNz, &inv, Lz_, nz, V, 2 * iNz, &zero, Y, nz) ==
-             CUBLAS_STATUS_SUCCESS;
+    k_pad_replicate<<<592, 256, 0, g_ops.st>>>(x, nz, nx, pad, P, iNz, (long long)plane);
+    bool ok = report(cudaGetLastError(), "k_pad_replicate");
+    // z transforms of the padded columns: A[x][kz]
+    BlueDesc d1 = dz_;
+    d1.in = P; d1.in_es = 1; d1.in_ss = Nz; d1.in_cplx = 0;
+    d1.out = A; d1.out_es = 1; d1.out_ss = Nz; d1.out_real = 0; d1.o0 = 0; d1.no = iNz;
+    d1.nseq = iNx; d1.dir = -1;
+    ok = ok && report(launch_bluestein(d1, g_ops.st), name);
+    // per z wavenumber: x transform, window W[kx][kz], inverse x transform at the model's columns
+    BlueDesc d2 = dx_;
+    d2.in = A; d2.in_es = Nz; d2.in_ss = 1; d2.in_cplx = 1;
+    d2.win = W; d2.win_es = Nz; d2.win_ss = 1;
+    d2.out = Gc; d2.out_es = Nz; d2.out_ss = 1; d2.out_real = 0; d2.o0 = pad; d2.no = nx;
+    d2.nseq = iNz; d2.dir = -1;
+    ok = ok && report(launch_bluestein(d2, g_ops.st), name);
+    // inverse z transforms of the model's columns at the model's rows, real part / (Nz Nx)
+    BlueDesc d3 = dz_;
+    d3.in = Gc; d3.in_es = 1; d3.in_ss = Nz; d3.in_cplx = 1;
+    d3.out = Y; d3.out_es = 1; d3.out_ss = nz; d3.out_real = 1; d3.divisor = (float)(iNz * iNx);
+    d3.o0 = pad; d3.no = nz; d3.nseq = nx; d3.dir = 1;
+    ok = ok && report(launch_bluestein(d3, g_ops.st), name);
     if (!ok) {
-        fprintf(stderr, "<error>: %s: GEMM failed\n", name);
         cudaStreamSynchronize(g_ops.st);
         return;
     }

@@ -405,6 +405,53 @@ void fwi_conv_spectrum_f64(const double *h, int n, int M, double *G)
     free(im);
 }
 
+void fwi_bluestein_tables(int N, int M, int f64, void *out)
+{
+    double *br = (double *)malloc(sizeof(double) * (size_t)N), *bi = (double *)malloc(sizeof(double) * (size_t)N);
+    for (int m = 0; m < N; m++) {
+        /* m^2 mod 2N keeps the angle small (the chirp has period 2N in m^2) */
+        const long long q = ((long long)m * m) % (2LL * N);
+        const double a = 3.141592653589793 * (double)q / N;
+        br[m] = cos(a);
+        bi[m] = sin(a);
+    }
+    double *re = (double *)calloc((size_t)M, sizeof(double)), *im = (double *)calloc((size_t)M, sizeof(double));
+    double *spec = (double *)malloc(sizeof(double) * 4 * (size_t)M);
+    for (int c = 0; c < 2; c++) {  /* c = 0: b, c = 1: conj(b) */
+        memset(re, 0, sizeof(double) * (size_t)M);
+        memset(im, 0, sizeof(double) * (size_t)M);
+        const double sg = c ? -1.0 : 1.0;
+        for (int m = 0; m < N; m++) {
+            re[m] = br[m];
+            im[m] = sg * bi[m];
+            if (m > 0) {
+                re[M - m] = br[m];
+                im[M - m] = sg * bi[m];
+            }
+        }
+        fft_pow2(re, im, M, -1);
+        for (int k = 0; k < M; k++) {
+            spec[(size_t)c * 2 * M + 2 * k] = re[k] / M;
+            spec[(size_t)c * 2 * M + 2 * k + 1] = im[k] / M;
+        }
+    }
+    const size_t n2 = 2 * (size_t)N;
+    if (f64) {
+        double *o = (double *)out;
+        for (int m = 0; m < N; m++) o[2 * m] = br[m], o[2 * m + 1] = bi[m];
+        memcpy(o + n2, spec, sizeof(double) * 4 * (size_t)M);
+    } else {
+        float *o = (float *)out;
+        for (int m = 0; m < N; m++) o[2 * m] = (float)br[m], o[2 * m + 1] = (float)bi[m];
+        for (size_t i = 0; i < 4 * (size_t)M; i++) o[n2 + i] = (float)spec[i];
+    }
+    free(br);
+    free(bi);
+    free(re);
+    free(im);
+    free(spec);
+}
+
 void fwi_fft_twiddles_f64(int M, double *tw)
 {
     for (int k = 0; k < M / 2; k++) {
@@ -525,115 +572,3 @@ void fwi_wavenumber_window(int filter, int Nx, int Nz, float dx, float dz, float
     free(kz);
 }
 
-/* cos and sin of 2 pi m / n, m = 0..n-1, FP64; entry (a b mod n) gives the DFT matrix element */
-typedef struct { double *c, *s; int n; } dft_table;
-
-static dft_table dft_table_make(int n)
-{
-    dft_table t = {(double *)malloc(sizeof(double) * (size_t)n), (double *)malloc(sizeof(double) * (size_t)n), n};
-    for (int m = 0; m < n; m++) {
-        t.c[m] = cos(2.0 * 3.141592653589793 * m / n);
-        t.s[m] = sin(2.0 * 3.141592653589793 * m / n);
-    }
-    return t;
-}
-
-static void dft_table_free(dft_table *t)
-{
-    free(t->c);
-    free(t->s);
-}
-
-static void dft_cs(const dft_table *t, long long a, long long b, double *c, double *sn)
-{
-    const int m = (int)((a * b) % t->n);
-    *c = t->c[m];
-    *sn = t->s[m];
-}
-
-/* padded index p of an n-sample line padded by `pad` replicated edge samples on each side */
-static int pad_source(int p, int pad, int n)
-{
-    int q = p - pad;
-    return q < 0 ? 0 : (q >= n ? n - 1 : q);
-}
-
-void fwi_wn_forward_z(int nz, int pad, float *A)
-{
-    const int Nz = nz + 2 * pad;
-    dft_table t = dft_table_make(Nz);
-    double *c = (double *)calloc((size_t)Nz * nz, sizeof(double)), *sn = (double *)calloc((size_t)Nz * nz, sizeof(double));
-    for (int p = 0; p < Nz; p++) {
-        const int b = pad_source(p, pad, nz);
-        for (int a = 0; a < Nz; a++) {
-            double cv, sv;
-            dft_cs(&t, a, p, &cv, &sv);
-            c[(size_t)b * Nz + a] += cv;
-            sn[(size_t)b * Nz + a] += sv;
-        }
-    }
-    for (size_t i = 0; i < (size_t)Nz * nz; i++) {
-        A[i] = (float)c[i];
-        A[(size_t)Nz * nz + i] = (float)-sn[i];
-    }
-    free(c);
-    free(sn);
-    dft_table_free(&t);
-}
-
-void fwi_wn_forward_x(int nx, int pad, float *R)
-{
-    const int Nx = nx + 2 * pad, ld = 2 * nx;
-    dft_table t = dft_table_make(Nx);
-    double *c = (double *)calloc((size_t)Nx * nx, sizeof(double)), *sn = (double *)calloc((size_t)Nx * nx, sizeof(double));
-    for (int p = 0; p < Nx; p++) {
-        const int b = pad_source(p, pad, nx);
-        for (int q = 0; q < Nx; q++) {
-            double cv, sv;
-            dft_cs(&t, q, p, &cv, &sv);
-            c[(size_t)q * nx + b] += cv; /* Cx' transposed: [b][q] at q * nx + b */
-            sn[(size_t)q * nx + b] += sv;
-        }
-    }
-    for (int q = 0; q < Nx; q++)
-        for (int b = 0; b < nx; b++) {
-            const float cv = (float)c[(size_t)q * nx + b], sv = (float)sn[(size_t)q * nx + b];
-            R[(size_t)q * ld + b] = cv;             /* [[C', -S'], [S', C']], column q < Nx */
-            R[(size_t)q * ld + nx + b] = sv;
-            R[(size_t)(Nx + q) * ld + b] = -sv;
-            R[(size_t)(Nx + q) * ld + nx + b] = cv;
-        }
-    free(c);
-    free(sn);
-    dft_table_free(&t);
-}
-
-void fwi_wn_inverse_x(int nx, int pad, float *R)
-{
-    const int Nx = nx + 2 * pad, ld = 2 * Nx;
-    dft_table t = dft_table_make(Nx);
-    for (int j = 0; j < nx; j++)
-        for (int q = 0; q < Nx; q++) {
-            double cv, sv;
-            dft_cs(&t, j + pad, q, &cv, &sv);
-            R[(size_t)j * ld + q] = (float)cv;              /* [[C^T, S^T], [-S^T, C^T]], column j < nx */
-            R[(size_t)j * ld + Nx + q] = (float)-sv;
-            R[(size_t)(nx + j) * ld + q] = (float)sv;
-            R[(size_t)(nx + j) * ld + Nx + q] = (float)cv;
-        }
-    dft_table_free(&t);
-}
-
-void fwi_wn_inverse_z(int nz, int pad, float *L)
-{
-    const int Nz = nz + 2 * pad;
-    dft_table t = dft_table_make(Nz);
-    for (int p = 0; p < Nz; p++)
-        for (int i = 0; i < nz; i++) {
-            double cv, sv;
-            dft_cs(&t, i + pad, p, &cv, &sv);
-            L[(size_t)p * nz + i] = (float)cv;               /* [C | -S] */
-            L[(size_t)(Nz + p) * nz + i] = (float)-sv;
-        }
-    dft_table_free(&t);
-}

@@ -69,24 +69,17 @@ void fwi_fft_twiddles(int M, float *tw);
 /* the same two tables in FP64 (for transforms that run in FP64) */
 void fwi_conv_spectrum_f64(const double *h, int n, int M, double *G);
 void fwi_fft_twiddles_f64(int M, double *tw);
+/* fwi_bluestein_tables: the tables of an N-point DFT computed as an M-point convolution
+ * (Bluestein; M = fwi_conv_size(N)): the chirp b_m = exp(i pi m^2 / N), m < N, then the spectra
+ * FFT_M(b wrapped) / M and FFT_M(conj(b) wrapped) / M (b is even in m, so b_{-m} = b_m sits at
+ * M - m), as (re, im) pairs: N + 2M complex values, FP64 (f64 != 0) or FP32. */
+void fwi_bluestein_tables(int N, int M, int f64, void *out);
 
 /* lowpass2d (filter 0, common.c:1042-1162) / bandpass2d (filter 1, :1164-1284) window over the
  * full Nx x Nz wavenumber plane of the padded field, W[ix * Nz + iz], from the reference's float
- * expressions (generate_frequency, common.c:333-361).
- *
- * The filter itself, Y = crop(IDFT2(W . DFT2(pad(X)))), runs as real GEMMs whose operators fold
- * the edge-replicating pad (pad_model2d, common.c:110-170) into the forward DFT and the crop into
- * the inverse one, all column-major with n = samples, N = n + 2 pad:
- *   fwi_wn_forward_z  A: two N x n blocks, C' and -S' (C' = cos(2 pi a p / N) summed over the padded
- *                        rows p that replicate sample b);
- *   fwi_wn_forward_x  R: 2n x 2N, [[C'^T, -S'^T], [S'^T, C'^T]];
- *   fwi_wn_inverse_x  R: 2N x 2n, [[C^T, S^T], [-S^T, C^T]] with C, S at the kept rows j + pad;
- *   fwi_wn_inverse_z  L: n x 2N, [C | -S] at the kept rows.  FP64, rounded once to float. */
+ * expressions (generate_frequency, common.c:333-361); the filter applies it between the 2-D DFTs
+ * of the padded field (Bluestein transforms on the device, fwi_bluestein_tables). */
 void fwi_wavenumber_window(int filter, int Nx, int Nz, float dx, float dz, float kpass, float kcut, float *W);
-void fwi_wn_forward_z(int nz, int pad, float *A);
-void fwi_wn_forward_x(int nx, int pad, float *R);
-void fwi_wn_inverse_x(int nx, int pad, float *R);
-void fwi_wn_inverse_z(int nz, int pad, float *L);
 
 #ifdef __cplusplus
 }

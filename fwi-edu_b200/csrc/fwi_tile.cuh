@@ -666,8 +666,19 @@ template <int TX, int NST, int MATH>
 __global__ void __launch_bounds__(TG * TX + 32, 3)
     k_tile_groups(const TileGroup *__restrict__ groups, int ngroups, long long L, int *err)
 {
-    int g = 0;
-    while (g + 1 < ngroups && (int)blockIdx.x >= groups[g + 1].b0) ++g;
+    // the block's group: the last one whose first block is at or before this one (b0 rises with
+    // the group index).  Each warp counts them 32 at a time with one load per lane and a ballot,
+    // instead of one dependent load per group.
+    int g = -1;
+    {
+        const int lane = (threadIdx.y * blockDim.x + threadIdx.x) & 31;
+        for (int base = 0; base < ngroups; base += 32) {
+            const int i = base + lane;
+            const bool le = i < ngroups && __ldg(&groups[i].b0) <= (int)blockIdx.x;
+            g += __popc(__ballot_sync(0xffffffffu, le));
+        }
+        g = max(g, 0);
+    }
     const TileGroup &T = groups[g];
     const long long Lg = L - T.L0;
     if (Lg < 0 || Lg >= T.nprog) return;

@@ -5,8 +5,8 @@ Pinned twice: against the reference's own output on a smoothed random field
 sources with FFTW) -- the in-place taper of the input bit for bit, the filtered field within
 rel-L2 1e-5 -- and against numpy's FFT run the way the reference runs FFTW (taper, edge-replicated
 pad, rfft2, the reference's float window on the stored half plane, irfft2, / (Nz Nx), crop) on
-other shapes, spacings and band edges.  The GPU computes the transforms as FP32 GEMMs with DFT
-operators that fold the pad and the crop.
+other shapes, spacings and band edges.  The GPU computes the DFTs of the padded field's own sizes
+as Bluestein transforms (hand-written FFT kernels, FP64 where a block holds the transform).
 """
 import ctypes as C
 import os
