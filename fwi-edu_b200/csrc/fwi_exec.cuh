@@ -46,8 +46,10 @@ struct fwi_exec {
     std::mutex mu;
     std::vector<ExecRun *> runs;      // in the batch
     std::vector<ExecRun *> finished;  // handed back, not yet polled
-    TileGroup *d_groups = nullptr;
+    TileGroup *d_groups = nullptr;  // the group table in global memory (more than GROUPS_PARAM groups)
     int groups_cap = 0;
+    GroupTable ptab;                  // the group table passed as a kernel parameter (at most GROUPS_PARAM)
+    bool use_param = false;
     bool dirty = true;
     int ngroups = 0;
     dim3 grid;
@@ -266,6 +268,15 @@ static int exec_table(fwi_exec *ex)
             t.push_back(T);
         }
     if (nb > 0x7fffffff) return fail(FWI_ERR_UNSUPPORTED, "too many blocks in one launch of the batch");
+    ex->use_param = (int)t.size() <= GROUPS_PARAM;
+    if (ex->use_param) {
+        memset(&ex->ptab, 0, sizeof(ex->ptab));
+        for (size_t i = 0; i < t.size(); i++) ex->ptab.g[i] = t[i];
+        ex->ngroups = (int)t.size();
+        ex->grid = dim3((unsigned)std::max<long long>(nb, 1), 1, 1);
+        ex->dirty = false;
+        return FWI_OK;
+    }
     if ((int)t.size() > ex->groups_cap) {
         if (ex->d_groups) {
             CK(cudaStreamSynchronize(ex->stream));
@@ -339,13 +350,23 @@ extern "C" int fwi_exec_step(fwi_exec *ex, int launches, int *active)
         lc.attrs = attr;
         lc.numAttrs = 1;
         const bool math = ex->math != 0;
-        auto fn = math ? k_tile_groups<EXEC_TX, EXEC_NST, 1> : k_tile_groups<EXEC_TX, EXEC_NST, 0>;
         static std::once_flag attr_once[2];
         std::call_once(attr_once[math ? 1 : 0], [&] {
-            cudaFuncSetAttribute((const void *)fn, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                 TileGeom<EXEC_TX>::smem(EXEC_NST));
+            const int sm = TileGeom<EXEC_TX>::smem(EXEC_NST);
+            cudaFuncSetAttribute(math ? (const void *)k_tile_groups<EXEC_TX, EXEC_NST, 1>
+                                      : (const void *)k_tile_groups<EXEC_TX, EXEC_NST, 0>,
+                                 cudaFuncAttributeMaxDynamicSharedMemorySize, sm);
+            cudaFuncSetAttribute(math ? (const void *)k_tile_groups_p<EXEC_TX, EXEC_NST, 1>
+                                      : (const void *)k_tile_groups_p<EXEC_TX, EXEC_NST, 0>,
+                                 cudaFuncAttributeMaxDynamicSharedMemorySize, sm);
         });
-        CK(cudaLaunchKernelEx(&lc, fn, (const TileGroup *)ex->d_groups, ex->ngroups, ex->L, ex->d_err));
+        if (ex->use_param) {
+            auto fn = math ? k_tile_groups_p<EXEC_TX, EXEC_NST, 1> : k_tile_groups_p<EXEC_TX, EXEC_NST, 0>;
+            CK(cudaLaunchKernelEx(&lc, fn, ex->ptab, ex->ngroups, ex->L, ex->d_err));
+        } else {
+            auto fn = math ? k_tile_groups<EXEC_TX, EXEC_NST, 1> : k_tile_groups<EXEC_TX, EXEC_NST, 0>;
+            CK(cudaLaunchKernelEx(&lc, fn, (const TileGroup *)ex->d_groups, ex->ngroups, ex->L, ex->d_err));
+        }
         ex->L++;
         ex->launches_total++;
         // runs whose pass ended with this launch: their work between passes, or hand-back

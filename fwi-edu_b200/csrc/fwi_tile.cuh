@@ -686,11 +686,51 @@ __global__ void __launch_bounds__(TG * TX + 32, 3)
     const int bx = l % (T.ntx + 1), rest = l / (T.ntx + 1);
     const int bz = rest % T.zt, row = rest / T.zt;
     const int by = T.halves == 2 ? row : 2 * row;
-    // the maps live in global memory, written before the launch: make them visible to the
-    // tensor-map proxy of this thread before its copies use them
-    asm volatile("fence.proxy.tensormap::generic.acquire.gpu [%0], 128;" ::"l"(&T.p1) : "memory");
-    asm volatile("fence.proxy.tensormap::generic.acquire.gpu [%0], 128;" ::"l"(&T.p0) : "memory");
-    asm volatile("fence.proxy.tensormap::generic.acquire.gpu [%0], 128;" ::"l"(&T.cf) : "memory");
+    // the maps live in global memory, written before the launch: the producer warp (the only
+    // one that issues tensor copies) makes them visible to its tensor-map proxy and brings them
+    // into the descriptor cache before its copies use them
+    if (threadIdx.y * TG + threadIdx.x >= TG * TX) {
+        asm volatile("fence.proxy.tensormap::generic.acquire.gpu [%0], 128;" ::"l"(&T.p1) : "memory");
+        asm volatile("fence.proxy.tensormap::generic.acquire.gpu [%0], 128;" ::"l"(&T.p0) : "memory");
+        asm volatile("fence.proxy.tensormap::generic.acquire.gpu [%0], 128;" ::"l"(&T.cf) : "memory");
+        asm volatile("prefetch.tensormap [%0];" ::"l"(&T.p1) : "memory");
+        asm volatile("prefetch.tensormap [%0];" ::"l"(&T.p0) : "memory");
+        asm volatile("prefetch.tensormap [%0];" ::"l"(&T.cf) : "memory");
+    }
+    tile_body<TX, NST, MATH, 1, 3>(T.p1, T.p0, T.cf, T.shots, T.prog, (int)Lg, T.shot_base, T.nshot, T.chunk, err,
+                                   bx, by, bz);
+}
+
+// The same launch with the group table as a kernel parameter (constant space, up to
+// GROUPS_PARAM groups: 24 KB of the 32 KB a launch may pass).  The tensor maps are then
+// parameters like those of the single-group kernels: no fences, no descriptor fetches from global
+// memory.
+constexpr int GROUPS_PARAM = 48;
+struct __align__(128) GroupTable {
+    TileGroup g[GROUPS_PARAM];
+};
+
+template <int TX, int NST, int MATH>
+__global__ void __launch_bounds__(TG * TX + 32, 3)
+    k_tile_groups_p(const __grid_constant__ GroupTable tab, int ngroups, long long L, int *err)
+{
+    int g = -1;
+    {
+        const int lane = (threadIdx.y * blockDim.x + threadIdx.x) & 31;
+        for (int base = 0; base < ngroups; base += 32) {
+            const int i = base + lane;
+            const bool le = i < ngroups && tab.g[i].b0 <= (int)blockIdx.x;
+            g += __popc(__ballot_sync(0xffffffffu, le));
+        }
+        g = max(g, 0);
+    }
+    const TileGroup &T = tab.g[g];
+    const long long Lg = L - T.L0;
+    if (Lg < 0 || Lg >= T.nprog) return;
+    const int l = (int)blockIdx.x - T.b0;
+    const int bx = l % (T.ntx + 1), rest = l / (T.ntx + 1);
+    const int bz = rest % T.zt, row = rest / T.zt;
+    const int by = T.halves == 2 ? row : 2 * row;
     tile_body<TX, NST, MATH, 1, 3>(T.p1, T.p0, T.cf, T.shots, T.prog, (int)Lg, T.shot_base, T.nshot, T.chunk, err,
                                    bx, by, bz);
 }
