@@ -683,8 +683,11 @@ __global__ void __launch_bounds__(TG * TX + 32, 3)
     const long long Lg = L - T.L0;
     if (Lg < 0 || Lg >= T.nprog) return;
     const int l = (int)blockIdx.x - T.b0;
+    // blocks in the single-group kernel's order: column tile fastest, then the row (chunk and
+    // item half), then the z tile (the surface tiles, whose epilogue is longest, start first)
+    const int rows = T.nblk / ((T.ntx + 1) * T.zt);
     const int bx = l % (T.ntx + 1), rest = l / (T.ntx + 1);
-    const int bz = rest % T.zt, row = rest / T.zt;
+    const int row = rest % rows, bz = rest / rows;
     const int by = T.halves == 2 ? row : 2 * row;
     // the maps live in global memory, written before the launch: the producer warp (the only
     // one that issues tensor copies) makes them visible to its tensor-map proxy and brings them
@@ -728,8 +731,11 @@ __global__ void __launch_bounds__(TG * TX + 32, 3)
     const long long Lg = L - T.L0;
     if (Lg < 0 || Lg >= T.nprog) return;
     const int l = (int)blockIdx.x - T.b0;
+    // blocks in the single-group kernel's order: column tile fastest, then the row (chunk and
+    // item half), then the z tile (the surface tiles, whose epilogue is longest, start first)
+    const int rows = T.nblk / ((T.ntx + 1) * T.zt);
     const int bx = l % (T.ntx + 1), rest = l / (T.ntx + 1);
-    const int bz = rest % T.zt, row = rest / T.zt;
+    const int row = rest % rows, bz = rest / rows;
     const int by = T.halves == 2 ? row : 2 * row;
     tile_body<TX, NST, MATH, 1, 3>(T.p1, T.p0, T.cf, T.shots, T.prog, (int)Lg, T.shot_base, T.nshot, T.chunk, err,
                                    bx, by, bz);
