@@ -141,7 +141,9 @@ struct fwi_ctx {
     std::map<std::string, cudaGraphExec_t> graphs;
     fwi_stats stats{};
     int math = 0;  // 0: bit-exact arithmetic, 1: contracted multiply-adds
-    int depth = 1;  // time steps per launch of the step kernel (1 or 2; FWI_DEPTH)
+    int depth = 1;  // time steps per launch of the step kernel (1 or 2): tuned per shape unless
+                    // FWI_DEPTH pins it
+    bool depth_pinned = false;
     bool use_graphs = true;  // capture the batched launch sequences as CUDA graphs
     bool pdl = true;         // consecutive steps as programmatic dependent launches
     bool tune = true;        // time the step kernel's launch shapes once per shape (autotune)
@@ -253,7 +255,10 @@ extern "C" int fwi_ctx_create(fwi_ctx **out, int device, size_t budget)
     c->device = device;
     c->budget = budget;
     if (const char *e = getenv("FWI_MATH")) c->math = atoi(e) ? 1 : 0;
-    if (const char *e = getenv("FWI_DEPTH")) c->depth = atoi(e) == 2 ? 2 : 1;
+    if (const char *e = getenv("FWI_DEPTH")) {
+        c->depth = atoi(e) == 2 ? 2 : 1;
+        c->depth_pinned = true;
+    }
     if (const char *e = getenv("FWI_GRAPH")) c->use_graphs = e[0] != '0';  // 0: direct launches (profilers)
     if (const char *e = getenv("FWI_PDL")) c->pdl = e[0] != '0';
     if (const char *e = getenv("FWI_TUNE")) c->tune = e[0] != '0';            // 0: heuristic launch shapes
@@ -1056,6 +1061,7 @@ struct TuneKey {
 };
 static std::mutex g_tune_mu;
 static std::map<TuneKey, TileCfg> g_tune;
+static std::map<TuneKey, float> g_tune_ms;  // the best shape's time for the tuner's forward steps
 
 // the heuristic shape, or the tuned one, with the environment's overrides applied last
 static TileCfg tile_config(fwi_ctx *c, const Plan *p, int nshot, bool batched, int depth = 1)
@@ -1169,6 +1175,26 @@ static int autotune(fwi_ctx *c, int shot_base, int nshot, const ShotRun *r0, boo
     TRY(check_kernel_error(c));
     std::lock_guard<std::mutex> lk(g_tune_mu);
     g_tune[key] = best;
+    g_tune_ms[key] = best_ms;
+    return FWI_OK;
+}
+
+// Halo depth as a tuned dimension: the first batched run of a shape tunes the one-step and the
+// two-step kernel on the same forward steps (the probes run before the pass that writes the
+// frames) and the context keeps the faster depth for its passes.  FWI_DEPTH pins the depth, and
+// so do the launch-shape overrides, a disabled tuner, snapshots and the comparison kernel.
+static int choose_depth(fwi_ctx *c, int shot_base, int nshot, const ShotRun *r0, bool batched)
+{
+    const char *ke = getenv("FWI_KERNEL");
+    if (c->depth_pinned || !batched || !c->tune || c->dump.verbose > 1 || (ke && strcmp(ke, "step") == 0) ||
+        getenv("FWI_TX") || getenv("FWI_NST") || getenv("FWI_CHUNK") || getenv("FWI_GPT") || getenv("FWI_OCC"))
+        return FWI_OK;
+    TRY(autotune(c, shot_base, nshot, r0, batched, 1));
+    TRY(autotune(c, shot_base, nshot, r0, batched, 2));
+    const Plan *p = r0->plan;
+    const TuneKey k1{p->Nx, p->G, nshot, c->math, 1, 1}, k2{p->Nx, p->G, nshot, c->math, 1, 2};
+    std::lock_guard<std::mutex> lk(g_tune_mu);
+    c->depth = g_tune_ms.count(k2) && g_tune_ms.count(k1) && g_tune_ms[k2] < g_tune_ms[k1] ? 2 : 1;
     return FWI_OK;
 }
 
@@ -2004,6 +2030,7 @@ static int run_forward_group(fwi_ctx *c, std::vector<ShotRun *> &rs, int problem
                              const std::string &gkey, int shot_base)
 {
     Program *prog;
+    TRY(choose_depth(c, shot_base, (int)rs.size(), rs[0], batched));
     TRY(forward_program(c, K_FWD0, &prog));
     for (ShotRun *r : rs) TRY(zero_initial(c, r, false));
     TRY(timed_program(c, 0, "fwd0/" + gkey, prog, shot_base, (int)rs.size(), rs[0], batched));
@@ -2021,6 +2048,7 @@ static int grad_forward(fwi_ctx *c, std::vector<ShotRun *> &rs, int precondition
                         const std::string &gkey, int shot_base)
 {
     Program *pf;
+    TRY(choose_depth(c, shot_base, (int)rs.size(), rs[0], batched));
     TRY(forward_program(c, K_FWD1, &pf));
     for (ShotRun *r : rs) TRY(zero_initial(c, r, true));
     TRY(timed_program(c, 0, "fwd1/" + gkey, pf, shot_base, (int)rs.size(), rs[0], batched));
