@@ -207,7 +207,9 @@ FWI_API int fwi_ctx_pass_stats(fwi_ctx *ctx, double *fwd_ms, long long *fwd_laun
 /* The step kernel's launch shape (tile width 8/16 columns, z-groups per thread, blocks per SM it
  * is compiled for, shared-memory ring depth 2..4 shots, shots per block) is picked by an
  * autotuner: the first run of a launch shape (padded grid, shots per launch, arithmetic, path)
- * times the candidates on the run's own scratch frames and keeps the fastest for the process.
+ * times the candidates on the run's own scratch frames and keeps the fastest for the process; on
+ * the batched path it also tunes the halo depth (one time step per launch, or two with the
+ * temporal-blocking kernel) and the context keeps the faster (FWI_DEPTH=1|2 pins it).
  * Off (or FWI_TUNE=0; or any of FWI_TX / FWI_NST / FWI_CHUNK / FWI_GPT / FWI_OCC set): a built-in
  * heuristic with those overrides.  fwi_ctx_launch_shape and fwi_ctx_launch_variant report the
  * shape of the last launch. */
