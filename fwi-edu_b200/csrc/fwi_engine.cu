@@ -148,6 +148,9 @@ struct fwi_ctx {
     bool pdl = true;         // consecutive steps as programmatic dependent launches
     bool tune = true;        // time the step kernel's launch shapes once per shape (autotune)
     bool wave = false;       // forward passes as one persistent wavefront launch where they fit (FWI_PERSIST=1)
+    bool fine = true;        // step launches wait for their neighbouring tiles only (TileSync; FWI_FINE=0: whole grid)
+    int *d_tflags = nullptr; // their completion flags
+    int tflags_cap = 0;
     int *d_wave = nullptr;   // its abort word and per-block item counters
     int wave_cap = 0;
     std::map<std::string, long long> graph_launches;  // kernels each captured graph holds
@@ -270,6 +273,9 @@ extern "C" int fwi_ctx_create(fwi_ctx **out, int device, size_t budget)
     if (const char *e = getenv("FWI_PERSIST")) c->wave = e[0] != '0';  // 1: forward passes as one wavefront launch
     c->wave_cap = 4096;  // abort word + one counter per resident block (148 SMs x a few blocks)
     TRY(dmalloc(c, (void **)&c->d_wave, c->wave_cap * sizeof(int)));
+    if (const char *e = getenv("FWI_FINE")) c->fine = e[0] != '0';
+    c->tflags_cap = 1 << 16;  // 2 halves x chunks x tiles; larger launches wait for the whole grid
+    TRY(dmalloc(c, (void **)&c->d_tflags, c->tflags_cap * sizeof(int)));
     *out = c;
     return FWI_OK;
 }
@@ -891,7 +897,7 @@ static LaunchCfg pick_launch(int Nx, int nshot, bool batched, int math)
 }
 
 typedef void (*TileFn)(const CUtensorMap, const CUtensorMap, const CUtensorMap, const ShotDesc *, const int4 *, int,
-                       int, int, int, int, int *);
+                       int, int, int, int, int *, const TileSync);
 
 template <int TX, int NST, int MATH, int GPT, int MINB>
 static TileFn tile_fn()
@@ -1023,7 +1029,12 @@ static int launch_tiles(fwi_ctx *c, const Program *prog, int L0, int L1, int sho
     int halves = 1;
     for (int L = L0; L < L1 && halves == 1; L++)
         if (prog->items[L].z != K_NONE) halves = 2;
-    dim3 grid(ntx + 1, halves * nchunks, zt);
+    // consecutive launches wait for their neighbouring tiles only (TileSync) where the flags fit
+    const size_t nflags = (size_t)2 * nchunks * zt * ntx;
+    const bool fine = c->fine && nflags <= (size_t)c->tflags_cap;
+    dim3 grid(fine ? ntx : ntx + 1, halves * nchunks, zt);
+    if (fine) CK(cudaMemsetAsync(c->d_tflags, 0, nflags * sizeof(int), c->stream));
+    TileSync ts{fine ? c->d_tflags : nullptr, -1, ntx, zt, halves};
     CUtensorMap m1, m0, mc;
     if (tx == 16) TRY(encode_group_maps<16>(r0->d, nshot, p->d_coef, &m1, &m0, &mc));
     else TRY(encode_group_maps<8>(r0->d, nshot, p->d_coef, &m1, &m0, &mc));
@@ -1043,7 +1054,8 @@ static int launch_tiles(fwi_ctx *c, const Program *prog, int L0, int L1, int sho
         const int4 &pw = prog->items[L];
         if (pw.x == K_NONE && pw.z == K_NONE) continue;
         CK(cudaLaunchKernelEx(&lc, fn, m1, m0, mc, (const ShotDesc *)c->d_desc, (const int4 *)prog->d, L, shot_base,
-                              nshot, chunk, halves, c->d_err));
+                              nshot, chunk, halves, c->d_err, ts));
+        ts.Lprev = L;
         c->launches++;
         if (c->snapping) TRY(snapshots_after(c, prog, L, shot_base, nshot));
     }

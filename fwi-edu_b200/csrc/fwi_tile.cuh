@@ -298,10 +298,70 @@ struct TileGeom {
 // thread the six coefficient float4s stay in registers for the chunk; 3 (k_tile3): they are read
 // from shared memory per shot instead, which fits three blocks per SM (more warps to hide
 // latency, at six more shared loads per group and shot).
+// How a step launch waits for the one before it.  flags == null: for the whole previous grid
+// (griddepcontrol.wait).  Otherwise for the 3 x 3 neighbouring tiles of the same chunk only: every
+// block stores, once its consumers have released all its stages (their stores precede that), the
+// program item it completed + 1 into flags[(by * zt + bz) * ntx + bx] (a gpu-scope fence first);
+// the producer of a block of item L polls the neighbours' flags for Lprev + 1 (both item halves
+// where the launches carry two), then fences (acquire, and the proxy fence for its tensor copies).
+// A programmatic dependent launch starts only once every block of the grid before it is resident,
+// so a block never waits for a block that cannot run.  The first launch of a pass (Lprev < 0)
+// waits for the whole previous grid.  In this mode the grid has no receiver-sampling column: the
+// tiles sample their receivers from the stage.
+struct TileSync {
+    int *flags;
+    int Lprev;        // program item of the previous launch of this pass, or -1
+    int ntx, zt;      // column and z tiles of the flag layout
+    int halves;       // 1 or 2 item halves carried by the launches
+};
+
+__device__ __forceinline__ int ld_relaxed(const int *p)
+{
+    int v;
+    asm volatile("ld.relaxed.gpu.global.s32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+    return v;
+}
+__device__ __forceinline__ void st_relaxed_gpu(int *p, int v)
+{
+    asm volatile("st.relaxed.gpu.global.s32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
+}
+
+// the producer's wait for the neighbours' previous item (TileSync); false when it ran out (2 s).
+// A set error word ends it at once: after one wait has run out, no launch of the pass waits again.
+__device__ __forceinline__ bool wait_neighbours(const TileSync &ts, int by, int bx, int bz, const int *err)
+{
+    int idx[18], cnt = 0;
+    for (int h = 0; h < ts.halves; ++h) {
+        const int row = ts.halves == 2 ? ((by & ~1) | h) : by;
+        for (int dz = -1; dz <= 1; ++dz)
+            for (int dx = -1; dx <= 1; ++dx) {
+                const int nz = bz + dz, nx = bx + dx;
+                if (nz >= 0 && nz < ts.zt && nx >= 0 && nx < ts.ntx) idx[cnt++] = (row * ts.zt + nz) * ts.ntx + nx;
+            }
+    }
+    const int need = ts.Lprev + 1;
+    const u64 t0 = global_ns();
+    bool ok = true;
+    for (;;) {
+        int mn = need;
+        for (int q = 0; q < cnt; ++q) mn = min(mn, ld_relaxed(ts.flags + idx[q]));
+        if (mn >= need) break;
+        if (global_ns() - t0 > 2000000000ull || ld_relaxed(err) != 0) {
+            ok = false;
+            break;
+        }
+        __nanosleep(64);
+    }
+    asm volatile("fence.acq_rel.gpu;" ::: "memory");
+    asm volatile("fence.proxy.async.global;" ::: "memory");
+    return ok;
+}
+
 template <int TX, int NST, int MATH, int GPT, int MINB>
 __device__ __forceinline__ void tile_body(const CUtensorMap &tm_p1, const CUtensorMap &tm_p0, const CUtensorMap &tm_cf,
                                           const ShotDesc *__restrict__ shots, const int4 *__restrict__ prog, int L,
-                                          int shot_base, int nshot, int chunk, int *err, int bx, int by, int bz)
+                                          int shot_base, int nshot, int chunk, int *err, int bx, int by, int bz,
+                                          const TileSync &ts)
 {
     using Geo = TileGeom<TX>;
     constexpr int NL = TG / GPT;  // consumer lanes per column
@@ -316,12 +376,30 @@ __device__ __forceinline__ void tile_body(const CUtensorMap &tm_p1, const CUtens
     __shared__ int s_isx[TILE_CH_MAX], s_isz[TILE_CH_MAX], s_rz0[TILE_CH_MAX], s_rz1[TILE_CH_MAX];
     __shared__ bool s_spec[TILE_CH_MAX];
     __shared__ int s_fi[2];  // frames of p1 and p0 (the same for every shot of the chunk)
+    // TileSync mode: trace row of this step's sample per shot (or null), and the receivers of the
+    // chunk's shots in the tile's columns and rows, (trace << 8) | (row - first row of the tile),
+    // -1 none, -2 several (read from the receiver list)
+    __shared__ float *s_tr[TILE_CH_MAX];
+    __shared__ int s_rcv[TILE_CH_MAX][TX];
 
     grid_dep_launch();  // the next step may begin its set-up once every block of this one runs
+    const bool fine = ts.flags != nullptr;
     const int4 pw = prog[L];
     const int kind = (by & 1) ? pw.z : pw.x;
     const int it = (by & 1) ? pw.w : pw.y;
-    if (kind == K_NONE) return;
+    if (kind == K_NONE) {
+        // an idle item half still completes its item in order, for the flags' readers
+        if (fine && threadIdx.x == 0 && threadIdx.y == 0) {
+            int *own = ts.flags + (by * ts.zt + bz) * ts.ntx + bx;
+            const u64 t0 = global_ns();
+            while (ts.Lprev >= 0 && ld_relaxed(own) < ts.Lprev + 1 && global_ns() - t0 < 2000000000ull &&
+                   ld_relaxed(err) == 0)
+                __nanosleep(64);
+            asm volatile("fence.acq_rel.gpu;" ::: "memory");
+            st_relaxed_gpu(own, L + 1);
+        }
+        return;
+    }
     const int cb = shot_base + (by >> 1) * chunk;
     const int n = min(chunk, shot_base + nshot - cb);
     if (n <= 0) return;
@@ -363,9 +441,17 @@ __device__ __forceinline__ void tile_body(const CUtensorMap &tm_p1, const CUtens
         step_frames(A, kind, it, i1, i0, io);  // the same frames for every shot of the chunk
         s_fi[0] = i1;
         s_fi[1] = i0;
-        grid_dep_wait();
-        mbar_arrive_expect(smem_u32(&cfbar), Geo::CF_BYTES);
-        tma_load3(smem_u32(smem), &tm_cf, 4 * G0, X0, 0, smem_u32(&cfbar));
+        if (fine && ts.Lprev >= 0) {
+            // the coefficients are the pass's own (the pass's first launch read them after waiting
+            // for everything before it): their copy overlaps the wait for the neighbours
+            mbar_arrive_expect(smem_u32(&cfbar), Geo::CF_BYTES);
+            tma_load3(smem_u32(smem), &tm_cf, 4 * G0, X0, 0, smem_u32(&cfbar));
+            if (!wait_neighbours(ts, by, bx, bz, err)) atomicExch(err, 1);
+        } else {
+            grid_dep_wait();
+            mbar_arrive_expect(smem_u32(&cfbar), Geo::CF_BYTES);
+            tma_load3(smem_u32(smem), &tm_cf, 4 * G0, X0, 0, smem_u32(&cfbar));
+        }
         for (; issued < min(n, NST); ++issued) {
             const unsigned b = smem_u32(&full[issued]);
             mbar_arrive_expect(b, Geo::P1_BYTES + Geo::P0_BYTES);
@@ -393,13 +479,35 @@ __device__ __forceinline__ void tile_body(const CUtensorMap &tm_p1, const CUtens
         const bool src_t = (fwd || kind == K_REP) && D.isx >= X0t && D.isx < X0t + TX && D.isz >= Z0t &&
                            D.isz < Z0t + 4 * TG;
         const bool inj_t = kind == K_ADJ && it >= 1 && Z0t + 4 * TG > D.rz0 && Z0t <= D.rz1;
-        s_spec[tid] = src_t || inj_t;
+        // TileSync mode: this tile samples the shot's receivers in its rows
+        float *tr = (fine && fwd && it % D.sr == 0) ? D.traces_t + (long long)(it / D.sr) * D.ntr : nullptr;
+        const bool smp_t = tr != nullptr && Z0t + 4 * TG > D.rz0 && Z0t <= D.rz1;
+        s_tr[tid] = smp_t ? tr : nullptr;
+        s_spec[tid] = src_t || inj_t || smp_t;
         spec_here = s_spec[tid];
+    }
+    if (fine && fwd && it % A.sr == 0 && warp < NW) {
+        // the receiver table of the chunk's shots in this tile (one pass of the consumers)
+        const int z_a = 4 * G0, z_b = 4 * G0 + 4 * TG - 1;
+        for (int q = tid; q < n * TX; q += NL * TX) {
+            const int sq = q / TX, kq = q - sq * TX, xq = X0 + kq;
+            const ShotDesc &D = shots[cb + sq];
+            int code = -1;
+            if (xq < Nx && D.rz1 >= z_a && D.rz0 <= z_b)
+                for (int e = D.colptr[xq]; e < D.colptr[xq + 1]; ++e) {
+                    const int2 r = D.rec[e];
+                    if (r.x < z_a || r.x > z_b) continue;
+                    code = code == -1 ? (r.y << 8) | (r.x - z_a) : -2;
+                }
+            s_rcv[sq][kq] = code;
+        }
     }
     // barriers and the per-shot scalars; no block-wide barrier follows.  any_spec: some shot of
     // the chunk has its source or receiver rows in this tile
     const bool any_spec = __syncthreads_or(spec_here) != 0;
-    grid_dep_wait();  // fields and accumulators: after the previous step (the producer waited already)
+    // fields and accumulators: after the previous step (the producer waited already; with
+    // TileSync the consumers touch them only after a stage the producer filled after its wait)
+    if (!fine || ts.Lprev < 0) grid_dep_wait();
 
     if (warp == NW) {
         // ---- producer: shot j into stage j % NST once every consumer warp has released that
@@ -424,6 +532,13 @@ __device__ __forceinline__ void tile_body(const CUtensorMap &tm_p1, const CUtens
         // them too, unless they gave up)
         mbar_wait(smem_u32(&cfbar), 0);
         for (int j = max(0, issued - NST); j < issued; ++j) mbar_wait(smem_u32(&full[j % NST]), (j / NST) & 1);
+        if (fine) {
+            // the item is complete once the consumers have released every stage (their stores come
+            // before their release): publish it
+            for (int j = max(0, n - NST); j < n; ++j) mbar_wait(smem_u32(&empty[j % NST]), (j / NST) & 1);
+            asm volatile("fence.acq_rel.gpu;" ::: "memory");
+            st_relaxed_gpu(ts.flags + (by * ts.zt + bz) * ts.ntx + bx, L + 1);
+        }
         return;
     }
 
@@ -503,6 +618,19 @@ __device__ __forceinline__ void tile_body(const CUtensorMap &tm_p1, const CUtens
                              const float4 &cq, const float4 &hi) {
         const int g = G0 + gl, z0 = 4 * g;
         if (g >= G || !xin) return;
+        if (fine && s_tr[i] != nullptr) {  // receivers sample u(t) before the step
+            const int code = s_rcv[i][k];
+            if (code >= 0) {
+                const int row = 4 * G0 + (code & 255);
+                if (row >= z0 && row < z0 + 4) s_tr[i][code >> 8] = comp(cq, row - z0);
+            } else if (code == -2) {
+                const ShotDesc &D = shots[cb + i];
+                for (int e = __ldg(D.colptr + x), e1 = __ldg(D.colptr + x + 1); e < e1; ++e) {
+                    const int2 r = __ldg(D.rec + e);
+                    if (r.x >= z0 && r.x < z0 + 4) s_tr[i][r.y] = comp(cq, r.x - z0);
+                }
+            }
+        }
         // above the free surface (rows < pml): never updated, stored or accumulated; the
         // mirrored rows pml-3..pml-1 are written by the groups that hold pml+1..pml+3
         if (A.fs && z0 + 3 < pml) return;
@@ -626,10 +754,10 @@ template <int TX, int NST, int MATH, int GPT>
 __global__ void __launch_bounds__(TG / GPT * TX + 32)
     k_tile(const __grid_constant__ CUtensorMap tm_p1, const __grid_constant__ CUtensorMap tm_p0,
            const __grid_constant__ CUtensorMap tm_cf, const ShotDesc *__restrict__ shots, const int4 *__restrict__ prog,
-           int L, int shot_base, int nshot, int chunk, int halves, int *err)
+           int L, int shot_base, int nshot, int chunk, int halves, int *err, const TileSync ts)
 {
     tile_body<TX, NST, MATH, GPT, 1>(tm_p1, tm_p0, tm_cf, shots, prog, L, shot_base, nshot, chunk, err, blockIdx.x,
-                                     halves == 2 ? blockIdx.y : 2 * blockIdx.y, blockIdx.z);
+                                     halves == 2 ? blockIdx.y : 2 * blockIdx.y, blockIdx.z, ts);
 }
 
 // the same step compiled for three blocks per SM, one group per thread, coefficients read from
@@ -638,10 +766,10 @@ template <int TX, int NST, int MATH>
 __global__ void __launch_bounds__(TG * TX + 32, 3)
     k_tile3(const __grid_constant__ CUtensorMap tm_p1, const __grid_constant__ CUtensorMap tm_p0,
             const __grid_constant__ CUtensorMap tm_cf, const ShotDesc *__restrict__ shots, const int4 *__restrict__ prog,
-            int L, int shot_base, int nshot, int chunk, int halves, int *err)
+            int L, int shot_base, int nshot, int chunk, int halves, int *err, const TileSync ts)
 {
     tile_body<TX, NST, MATH, 1, 3>(tm_p1, tm_p0, tm_cf, shots, prog, L, shot_base, nshot, chunk, err, blockIdx.x,
-                                   halves == 2 ? blockIdx.y : 2 * blockIdx.y, blockIdx.z);
+                                   halves == 2 ? blockIdx.y : 2 * blockIdx.y, blockIdx.z, ts);
 }
 
 // ------------------------------------------------------------ several groups in one launch
@@ -701,7 +829,7 @@ __global__ void __launch_bounds__(TG * TX + 32, 3)
         asm volatile("prefetch.tensormap [%0];" ::"l"(&T.cf) : "memory");
     }
     tile_body<TX, NST, MATH, 1, 3>(T.p1, T.p0, T.cf, T.shots, T.prog, (int)Lg, T.shot_base, T.nshot, T.chunk, err,
-                                   bx, by, bz);
+                                   bx, by, bz, TileSync{nullptr, -1, 0, 0, 1});
 }
 
 // The same launch with the group table as a kernel parameter (constant space, up to
@@ -738,7 +866,7 @@ __global__ void __launch_bounds__(TG * TX + 32, 3)
     const int row = rest % rows, bz = rest / rows;
     const int by = T.halves == 2 ? row : 2 * row;
     tile_body<TX, NST, MATH, 1, 3>(T.p1, T.p0, T.cf, T.shots, T.prog, (int)Lg, T.shot_base, T.nshot, T.chunk, err,
-                                   bx, by, bz);
+                                   bx, by, bz, TileSync{nullptr, -1, 0, 0, 1});
 }
 
 }  // namespace fwi
