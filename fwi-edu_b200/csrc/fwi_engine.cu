@@ -1029,9 +1029,11 @@ static int launch_tiles(fwi_ctx *c, const Program *prog, int L0, int L1, int sho
     int halves = 1;
     for (int L = L0; L < L1 && halves == 1; L++)
         if (prog->items[L].z != K_NONE) halves = 2;
-    // consecutive launches wait for their neighbouring tiles only (TileSync) where the flags fit
+    // consecutive launches wait for their neighbouring tiles only (TileSync) where the flags fit;
+    // a one-shot launch (the plain path) is a few microseconds long, too short for the flags' fences
+    // and polls to pay off, and waits for the whole grid before it
     const size_t nflags = (size_t)2 * nchunks * zt * ntx;
-    const bool fine = c->fine && nflags <= (size_t)c->tflags_cap;
+    const bool fine = c->fine && nshot >= 2 && nflags <= (size_t)c->tflags_cap;
     dim3 grid(fine ? ntx : ntx + 1, halves * nchunks, zt);
     if (fine) CK(cudaMemsetAsync(c->d_tflags, 0, nflags * sizeof(int), c->stream));
     TileSync ts{fine ? c->d_tflags : nullptr, -1, ntx, zt, halves};
