@@ -24,6 +24,8 @@ struct ExecGroup {
     CUtensorMap p1, p0, cf;
     const Program *prog = nullptr;
     long long L0 = 0;
+    int *flags = nullptr;  // the group's TileSync flags in its context's flag array, or null
+    size_t nflags = 0;
 };
 
 struct ExecRun {
@@ -111,6 +113,10 @@ static int exec_setup(fwi_ctx *c, ExecRun *er)
         eg.prog = pf;
         er->groups.push_back(eg);
     }
+    // Neighbour waits between the launches (TileSync) would need the group's flags here, zeroed
+    // at the start of each pass; they are left off: measured on one 60-shot gradient run they made
+    // the executor slower (166 -> 172 ms) and the serving mix too, while the single-run launches
+    // gain 8 % from them.  The groups wait for the whole launch before (flags null).
     // cell updates of the run, as fwi_ctx_run counts them
     er->cells = 0.0;
     for (int i = 0; i < ns; i++) {
@@ -146,6 +152,7 @@ static int exec_forward_done(fwi_exec *ex, ExecRun *er)
             TRY(adj_init(c, rs, g.shot_base));
             g.prog = &c->progs.at("adj/overlap");
             g.L0 = ex->L;
+            if (g.flags) CK(cudaMemsetAsync(g.flags, 0, g.nflags * sizeof(int), ex->stream));
         }
     }
     return FWI_OK;
@@ -262,8 +269,9 @@ static int exec_table(fwi_exec *ex)
             T.ntx = g.ntx;
             T.zt = g.zt;
             T.halves = er->phase == 1 ? 2 : 1;  // the adjoint program pairs replay and adjoint items
+            T.flags = g.flags;
             T.b0 = (int)nb;
-            T.nblk = (g.ntx + 1) * g.zt * T.halves * ((g.nshot + g.chunk - 1) / g.chunk);
+            T.nblk = (g.flags ? g.ntx : g.ntx + 1) * g.zt * T.halves * ((g.nshot + g.chunk - 1) / g.chunk);
             nb += T.nblk;
             t.push_back(T);
         }

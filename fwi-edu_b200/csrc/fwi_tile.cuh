@@ -788,7 +788,24 @@ struct __align__(128) TileGroup {
     int b0, nblk;                 // first block and blocks of the group
     int ntx, zt;                  // column tiles (ntx: the receiver-sampling column) and z tiles
     int halves;                   // 1: the program uses item halves .x only (forward); 2: both
+    int *flags;                   // non-null: neighbour waits (TileSync) over the group's own flags,
+                                  // no sampling column; null: whole-grid waits
 };
+
+// the group's block l as (column tile, row, z tile) in the single-group grid's order (column tile
+// fastest, then the chunk and item half, then the z tile), and its TileSync
+__device__ __forceinline__ void group_block(const TileGroup &T, long long Lg, int l, int &bx, int &by, int &bz,
+                                            TileSync &ts)
+{
+    const int cols = T.flags ? T.ntx : T.ntx + 1;
+    const int rows = T.nblk / (cols * T.zt);
+    bx = l % cols;
+    const int rest = l / cols;
+    const int row = rest % rows;
+    bz = rest / rows;
+    by = T.halves == 2 ? row : 2 * row;
+    ts = TileSync{T.flags, Lg > 0 ? (int)Lg - 1 : -1, T.ntx, T.zt, T.halves};
+}
 
 template <int TX, int NST, int MATH>
 __global__ void __launch_bounds__(TG * TX + 32, 3)
@@ -811,12 +828,11 @@ __global__ void __launch_bounds__(TG * TX + 32, 3)
     const long long Lg = L - T.L0;
     if (Lg < 0 || Lg >= T.nprog) return;
     const int l = (int)blockIdx.x - T.b0;
-    // blocks in the single-group kernel's order: column tile fastest, then the row (chunk and
-    // item half), then the z tile (the surface tiles, whose epilogue is longest, start first)
-    const int rows = T.nblk / ((T.ntx + 1) * T.zt);
-    const int bx = l % (T.ntx + 1), rest = l / (T.ntx + 1);
-    const int row = rest % rows, bz = rest / rows;
-    const int by = T.halves == 2 ? row : 2 * row;
+    // blocks in the single-group kernel's order (the surface tiles, whose epilogue is longest,
+    // start first)
+    int bx, by, bz;
+    TileSync ts;
+    group_block(T, Lg, l, bx, by, bz, ts);
     // the maps live in global memory, written before the launch: the producer warp (the only
     // one that issues tensor copies) makes them visible to its tensor-map proxy and brings them
     // into the descriptor cache before its copies use them
@@ -829,7 +845,7 @@ __global__ void __launch_bounds__(TG * TX + 32, 3)
         asm volatile("prefetch.tensormap [%0];" ::"l"(&T.cf) : "memory");
     }
     tile_body<TX, NST, MATH, 1, 3>(T.p1, T.p0, T.cf, T.shots, T.prog, (int)Lg, T.shot_base, T.nshot, T.chunk, err,
-                                   bx, by, bz, TileSync{nullptr, -1, 0, 0, 1});
+                                   bx, by, bz, ts);
 }
 
 // The same launch with the group table as a kernel parameter (constant space, up to
@@ -859,14 +875,13 @@ __global__ void __launch_bounds__(TG * TX + 32, 3)
     const long long Lg = L - T.L0;
     if (Lg < 0 || Lg >= T.nprog) return;
     const int l = (int)blockIdx.x - T.b0;
-    // blocks in the single-group kernel's order: column tile fastest, then the row (chunk and
-    // item half), then the z tile (the surface tiles, whose epilogue is longest, start first)
-    const int rows = T.nblk / ((T.ntx + 1) * T.zt);
-    const int bx = l % (T.ntx + 1), rest = l / (T.ntx + 1);
-    const int row = rest % rows, bz = rest / rows;
-    const int by = T.halves == 2 ? row : 2 * row;
+    // blocks in the single-group kernel's order (the surface tiles, whose epilogue is longest,
+    // start first)
+    int bx, by, bz;
+    TileSync ts;
+    group_block(T, Lg, l, bx, by, bz, ts);
     tile_body<TX, NST, MATH, 1, 3>(T.p1, T.p0, T.cf, T.shots, T.prog, (int)Lg, T.shot_base, T.nshot, T.chunk, err,
-                                   bx, by, bz, TileSync{nullptr, -1, 0, 0, 1});
+                                   bx, by, bz, ts);
 }
 
 }  // namespace fwi
