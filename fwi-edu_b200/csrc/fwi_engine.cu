@@ -149,6 +149,11 @@ struct fwi_ctx {
     bool tune = true;        // time the step kernel's launch shapes once per shape (autotune)
     bool wave = false;       // forward passes as one persistent wavefront launch where they fit (FWI_PERSIST=1)
     bool fine = true;        // step launches wait for their neighbouring tiles only (TileSync; FWI_FINE=0: whole grid)
+    // the observed gathers go up on a stream of their own, overlapping the forward pass; the
+    // residual waits for them (ev_obs) the first time it reads them
+    cudaStream_t xstream = nullptr;
+    cudaEvent_t ev_obs = nullptr, ev_tail = nullptr;
+    bool obs_pending = false;
     int *d_tflags = nullptr; // their completion flags
     int tflags_cap = 0;
     int *d_wave = nullptr;   // its abort word and per-block item counters
@@ -225,6 +230,17 @@ static void dfree(fwi_ctx *c, void *p, size_t = 0)
     cudaFreeAsync(p, c->stream);
 }
 
+// the main stream waits for the observed gathers' upload (before the residual reads them, or
+// before their buffers are freed)
+static int obs_join(fwi_ctx *c)
+{
+    if (!c->obs_pending) return FWI_OK;
+    cudaError_t e = cudaStreamWaitEvent(c->stream, c->ev_obs, 0);
+    if (e != cudaSuccess) return fail(FWI_ERR_CUDA, "cudaStreamWaitEvent: %s", cudaGetErrorString(e));
+    c->obs_pending = false;
+    return FWI_OK;
+}
+
 static void free_run(fwi_ctx *c, ShotRun *r)
 {
     for (void *p : r->allocs) dfree(c, p);
@@ -266,6 +282,9 @@ extern "C" int fwi_ctx_create(fwi_ctx **out, int device, size_t budget)
     if (const char *e = getenv("FWI_PDL")) c->pdl = e[0] != '0';
     if (const char *e = getenv("FWI_TUNE")) c->tune = e[0] != '0';            // 0: heuristic launch shapes
     CK(cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking));
+    CK(cudaStreamCreateWithFlags(&c->xstream, cudaStreamNonBlocking));
+    CK(cudaEventCreateWithFlags(&c->ev_obs, cudaEventDisableTiming));
+    CK(cudaEventCreateWithFlags(&c->ev_tail, cudaEventDisableTiming));
     CK(cudaEventCreate(&c->ev0));
     CK(cudaEventCreate(&c->ev1));
     TRY(dmalloc(c, (void **)&c->d_err, sizeof(int)));
@@ -284,6 +303,7 @@ extern "C" int fwi_ctx_destroy(fwi_ctx *c)
 {
     if (!c) return FWI_OK;
     cudaSetDevice(c->device);
+    obs_join(c);
     cudaStreamSynchronize(c->stream);
     free_runs(c);
     for (auto &p : c->plans) fwi_free_coefs(&p->hc);
@@ -297,6 +317,10 @@ extern "C" int fwi_ctx_destroy(fwi_ctx *c)
             cudaEventDestroy(e.first);
             cudaEventDestroy(e.second);
         }
+    cudaStreamSynchronize(c->xstream);
+    cudaStreamDestroy(c->xstream);
+    cudaEventDestroy(c->ev_obs);
+    cudaEventDestroy(c->ev_tail);
     cudaStreamDestroy(c->stream);
     delete c;
     return FWI_OK;
@@ -398,6 +422,7 @@ extern "C" int fwi_ctx_set_shots(fwi_ctx *c, const fwi_shot *shots, int nshot)
             if (!in_fd_range(s.igx[r], s.igz[r], c->nz, nxx, c->pml, c->fs))
                 return fail(FWI_ERR_ARG, "shot %d: receiver %d (%d,%d) outside the updated grid", i, r, s.igx[r], s.igz[r]);
     }
+    TRY(obs_join(c));
     free_runs(c);
     for (float *p : c->d_obs) dfree(c, p, 0);
     for (float *p : c->d_pre) dfree(c, p, 0);
@@ -436,11 +461,17 @@ extern "C" int fwi_ctx_set_observed(fwi_ctx *c, const float *const *obs)
 {
     if (!c || !obs) return fail(FWI_ERR_ARG, "NULL argument");
     CK(cudaSetDevice(c->device));
-    for (size_t i = 0; i < c->shots.size(); i++) {
+    for (size_t i = 0; i < c->shots.size(); i++)
         if (!obs[i]) return fail(FWI_ERR_ARG, "observed gather %zu is NULL", i);
+    // after everything issued so far (a run still reading the previous gathers), beside what
+    // comes next: the residual waits for the copies (gather)
+    CK(cudaEventRecord(c->ev_tail, c->stream));
+    CK(cudaStreamWaitEvent(c->xstream, c->ev_tail, 0));
+    for (size_t i = 0; i < c->shots.size(); i++)
         CK(cudaMemcpyAsync(c->d_obs[i], obs[i], (size_t)c->shots[i].s.ntr * c->shots[i].s.ns * 4,
-                           cudaMemcpyHostToDevice, c->stream));
-    }
+                           cudaMemcpyHostToDevice, c->xstream));
+    CK(cudaEventRecord(c->ev_obs, c->xstream));
+    c->obs_pending = true;
     return FWI_OK;
 }
 
@@ -1595,6 +1626,7 @@ static int reduce(fwi_ctx *c, std::vector<SumDesc> sd, std::vector<double> &out_
 // ---------------------------------------------------------------- runs
 static int gather(fwi_ctx *c, const std::vector<ShotRun *> &rs, int mode, bool with_adj, bool trace_taper = true)
 {
+    if (mode == 1) TRY(obs_join(c));  // the residual reads the observed gathers
     std::vector<GatherDesc> gd;
     int maxns = 1, maxtr = 1;
     for (ShotRun *r : rs) {
