@@ -645,6 +645,7 @@ static int prepare_run(fwi_ctx *c, ShotRun *r, int shot, bool gradient)
     d.S5 = d.d / MST + 2;
     d.isx = s.isx + c->pml; d.isz = s.isz + c->pml;
     d.invdx = hc.invdx; d.invdz = hc.invdz; d.invdxdx = hc.invdxdx; d.invdzdz = hc.invdzdz;
+    d.negzero = -0.0f;
     d.invdtdt = hc.invdtdt; d.dt = c->dt;
     const size_t fr = p->frame();
     d.frame = (long long)fr;

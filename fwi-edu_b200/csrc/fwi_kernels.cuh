@@ -27,6 +27,7 @@ struct ShotDesc {
     int nt, d, K, ns, sr, ntr, S5, hessian;
     int isx, isz;  // padded source cell
     float invdx, invdz, invdxdx, invdzdz, invdtdt, dt;
+    float negzero;  // -0.0f, for the step kernels' packed products (fma(a, b, -0) rounds as a*b)
     // coefficients [Nx][ld]
     const float *c1, *c2, *ck, *irx, *irz, *ir;
     // source terms per step: forward (double, propagation.c:558) and replay (float, :662)

@@ -81,14 +81,15 @@ __device__ __forceinline__ u64 fma2(u64 a, u64 b, u64 c)
 constexpr float FD_C1 = 0.77793115f, FD_C2 = -0.17388691f, FD_C3 = 0.02338713f;
 constexpr float FD_D0 = -2.8215452f, FD_D1 = 1.57663238f, FD_D2 = -0.18347238f, FD_D3 = 0.01761260f;
 
-// the stencil constants and grid spacings as packed pairs (the contracted path), and the spacings
-// as scalars (the exact path, whose products are scalar multiplies: the constants enter them as
-// immediates and hold no registers)
+// the stencil constants and grid spacings as packed pairs (the contracted path uses them all; the
+// exact path multiplies by the stencil constants as scalar immediates, which hold no registers), and
+// -0 as a pair: NZ, the addend of the exact path's packed products, read at run time (negzero) so
+// that the compiler cannot drop it
 struct PkConst {
-    u64 C1, C2, C3, D0, D1, D2, D3, idx, idz, idxx, idzz;
-    float sidxx, sidzz;
+    u64 C1, C2, C3, D0, D1, D2, D3, idx, idz, idxx, idzz, NZ;
 };
-__device__ __forceinline__ PkConst make_pkconst(float invdx, float invdz, float invdxdx, float invdzdz)
+__device__ __forceinline__ PkConst make_pkconst(float invdx, float invdz, float invdxdx, float invdzdz,
+                                                float negzero)
 {
     PkConst K;
     K.C1 = pk(FD_C1, FD_C1);
@@ -102,26 +103,24 @@ __device__ __forceinline__ PkConst make_pkconst(float invdx, float invdz, float 
     K.idz = pk(invdz, invdz);
     K.idxx = pk(invdxdx, invdxdx);
     K.idzz = pk(invdzdz, invdzdz);
-    K.sidxx = invdxdx;
-    K.sidzz = invdzdz;
+    K.NZ = pk(negzero, negzero);
     return K;
 }
 
 // Two vertically adjacent cells of one column: propagation.c:13-74 with each product and sum
-// rounded on its own, in the reference's order.  The exact path (MATH 0) rounds every product
-// on its own with two scalar multiplies (__fmul_rn is never contracted; a packed multiply would
-// be fused by the compiler into the following packed add although both carry .rn); the sums stay
-// packed.
+// rounded on its own, in the reference's order.  The exact path (MATH 0) must round every product
+// that feeds a sum on its own, and a packed multiply would be fused by the compiler into the packed
+// add that follows although both carry .rn.  So a product by a stencil constant is two scalar
+// multiplies by an immediate (__fmul_rn is never contracted), and a product of two fields is one
+// packed fma(a, b, -0): a*b + (-0) rounds exactly as a*b, signed zeros included, and an fma is not
+// fused any further.  The sums stay packed.
 template <int MATH>
 __device__ __forceinline__ u64 cell2(u64 zm3, u64 zm2, u64 zm1, u64 z0, u64 zp1, u64 zp2, u64 zp3, u64 xm3, u64 xm2,
                                      u64 xm1, u64 xp1, u64 xp2, u64 xp3, u64 c1, u64 c2, u64 ck, u64 irx, u64 irz,
                                      u64 ir, u64 p0, const PkConst &k)
 {
     if (MATH == 0) {
-        auto mul = [&](u64 a, u64 b) {
-            const float2 x = upk(a), y = upk(b);
-            return pk(__fmul_rn(x.x, y.x), __fmul_rn(x.y, y.y));
-        };
+        auto mul = [&](u64 a, u64 b) { return fma2(a, b, k.NZ); };
         auto mulk = [&](float c, u64 b) {
             const float2 y = upk(b);
             return pk(__fmul_rn(c, y.x), __fmul_rn(c, y.y));
@@ -134,9 +133,9 @@ __device__ __forceinline__ u64 cell2(u64 zm3, u64 zm2, u64 zm1, u64 z0, u64 zp1,
             mul2(add2(add2(mulk(FD_C1, sub2(xp1, xm1)), mulk(FD_C2, sub2(xp2, xm2))), mulk(FD_C3, sub2(xp3, xm3))),
                  k.idx);
         const u64 d0 = mulk(FD_D0, z0);
-        const u64 dzz = mulk(k.sidzz, add2(add2(add2(d0, mulk(FD_D1, add2(zp1, zm1))), mulk(FD_D2, add2(zp2, zm2))),
+        const u64 dzz = mul(k.idzz, add2(add2(add2(d0, mulk(FD_D1, add2(zp1, zm1))), mulk(FD_D2, add2(zp2, zm2))),
                                            mulk(FD_D3, add2(zp3, zm3))));
-        const u64 dxx = mulk(k.sidxx, add2(add2(add2(d0, mulk(FD_D1, add2(xp1, xm1))), mulk(FD_D2, add2(xp2, xm2))),
+        const u64 dxx = mul(k.idxx, add2(add2(add2(d0, mulk(FD_D1, add2(xp1, xm1))), mulk(FD_D2, add2(xp2, xm2))),
                                            mulk(FD_D3, add2(xp3, xm3))));
         const u64 lap = add2(add2(mul(irx, dpdx), mul(irz, dpdz)), mul(ir, add2(dxx, dzz)));
         return add2(add2(mul(c1, z0), mul(c2, p0)), mul(ck, lap));
@@ -564,7 +563,7 @@ __device__ __forceinline__ void tile_body(const CUtensorMap &tm_p1, const CUtens
     const bool acc_tile = hess || image;
     const long long colx = (long long)x * A.ld;
     const float invdx = A.invdx, invdz = A.invdz, invdtdt = A.invdtdt;
-    const PkConst K = make_pkconst(invdx, invdz, A.invdxdx, A.invdzdz);
+    const PkConst K = make_pkconst(invdx, invdz, A.invdxdx, A.invdzdz, A.negzero);
     const float4 zero4 = make_float4(0.f, 0.f, 0.f, 0.f);
     const float4(*scf)[TX][TG] = reinterpret_cast<const float4(*)[TX][TG]>(smem);
     constexpr bool CF_REG = GPT == 1 && MINB < 3;

@@ -175,7 +175,7 @@ __global__ void __launch_bounds__(TG * TX + 32, 2)
     const int zlo = A.izStart, zhi = Nz - 4;
     const int fs_hi = min(2 * pml, pml + 3);  // last mirrored source row (snapshot steps use the one-step kernel)
     const float invdx = A.invdx, invdz = A.invdz, invdtdt = A.invdtdt;
-    const PkConst K = make_pkconst(invdx, invdz, A.invdxdx, A.invdzdz);
+    const PkConst K = make_pkconst(invdx, invdz, A.invdxdx, A.invdzdz, A.negzero);
     const float4 zero4 = make_float4(0.f, 0.f, 0.f, 0.f);
     // shared-memory addresses: coefficient plane f, grown-region column c, group g
     auto cf_at = [&](int f, int c, int g) { return sm0 + (unsigned)(((f * Geo::CX + c) * Geo::CG + g) * 16); };

@@ -308,7 +308,7 @@ __global__ void __launch_bounds__(TG * WAVE_TX + 32, 3)
     const bool fs_tile = A.fs && 4 * G0 <= fs_hi;
     const long long colx = (long long)x * A.ld;
     const float invdtdt = A.invdtdt;
-    const PkConst K = make_pkconst(A.invdx, A.invdz, A.invdxdx, A.invdzdz);
+    const PkConst K = make_pkconst(A.invdx, A.invdz, A.invdxdx, A.invdzdz, A.negzero);
     const float4 zero4 = make_float4(0.f, 0.f, 0.f, 0.f);
     const float4(*scf)[TX][TG] = reinterpret_cast<const float4(*)[TX][TG]>(smem);
     const int gl = zl, g = G0 + gl, z0 = 4 * g;
