@@ -380,6 +380,10 @@ __device__ __forceinline__ void tile_body(const CUtensorMap &tm_p1, const CUtens
     // -1 none, -2 several (read from the receiver list)
     __shared__ float *s_tr[TILE_CH_MAX];
     __shared__ int s_rcv[TILE_CH_MAX][TX];
+    // adjoint steps: the same table for the injection, with each receiver's interpolation weight
+    // (recK) and the step's adjoint-source row per shot
+    __shared__ float s_rk[TILE_CH_MAX][TX];
+    __shared__ const float *s_adj[TILE_CH_MAX];
 
     grid_dep_launch();  // the next step may begin its set-up once every block of this one runs
     const bool fine = ts.flags != nullptr;
@@ -482,23 +486,30 @@ __device__ __forceinline__ void tile_body(const CUtensorMap &tm_p1, const CUtens
         float *tr = (fine && fwd && it % D.sr == 0) ? D.traces_t + (long long)(it / D.sr) * D.ntr : nullptr;
         const bool smp_t = tr != nullptr && Z0t + 4 * TG > D.rz0 && Z0t <= D.rz1;
         s_tr[tid] = smp_t ? tr : nullptr;
+        s_adj[tid] = inj_t ? D.adj_t + (long long)(it - 1) * D.ntr : nullptr;
         s_spec[tid] = src_t || inj_t || smp_t;
         spec_here = s_spec[tid];
     }
-    if (fine && fwd && it % A.sr == 0 && warp < NW) {
-        // the receiver table of the chunk's shots in this tile (one pass of the consumers)
+    const bool inj_tab = kind == K_ADJ && it >= 1;
+    if (((fine && fwd && it % A.sr == 0) || inj_tab) && warp < NW) {
+        // the receiver table of the chunk's shots in this tile (one pass of the consumers): for
+        // the receiver sampling of a forward step, or the adjoint injection, so that a shot's
+        // step finds its receivers without a chain of dependent loads
         const int z_a = 4 * G0, z_b = 4 * G0 + 4 * TG - 1;
         for (int q = tid; q < n * TX; q += NL * TX) {
             const int sq = q / TX, kq = q - sq * TX, xq = X0 + kq;
             const ShotDesc &D = shots[cb + sq];
             int code = -1;
+            float rk = 0.0f;
             if (xq < Nx && D.rz1 >= z_a && D.rz0 <= z_b)
                 for (int e = D.colptr[xq]; e < D.colptr[xq + 1]; ++e) {
                     const int2 r = D.rec[e];
                     if (r.x < z_a || r.x > z_b) continue;
                     code = code == -1 ? (r.y << 8) | (r.x - z_a) : -2;
+                    if (inj_tab) rk = D.recK[e];
                 }
             s_rcv[sq][kq] = code;
+            if (inj_tab) s_rk[sq][kq] = rk;
         }
     }
     // barriers and the per-shot scalars; no block-wide barrier follows.  any_spec: some shot of
@@ -633,6 +644,18 @@ __device__ __forceinline__ void tile_body(const CUtensorMap &tm_p1, const CUtens
         // above the free surface (rows < pml): never updated, stored or accumulated; the
         // mirrored rows pml-3..pml-1 are written by the groups that hold pml+1..pml+3
         if (A.fs && z0 + 3 < pml) return;
+        // adjoint injection of a tile column with one receiver: its sample is loaded first, so
+        // that the load overlaps the stencil
+        const int code_inj = inject ? s_rcv[i][k] : -1;
+        int inj_j = -1;
+        float adjv = 0.0f;
+        if (code_inj >= 0) {
+            const int row = 4 * G0 + (code_inj & 255);
+            if (row >= z0 && row < z0 + 4) {
+                inj_j = row - z0;
+                adjv = __ldg(s_adj[i] + (code_inj >> 8));
+            }
+        }
         float4 p0;
         float4 v = group_value(sb, gl, lo, cq, hi, p0);
         const long long col = colx + z0;
@@ -666,7 +689,14 @@ __device__ __forceinline__ void tile_body(const CUtensorMap &tm_p1, const CUtens
             acc[0] = make_double2(a[0], a[1]);
             acc[1] = make_double2(a[2], a[3]);
         }
-        if (inject && z0 + 3 >= s_rz0[i] && z0 <= s_rz1[i]) {
+        if (inject && z0 + 3 >= s_rz0[i] && z0 <= s_rz1[i] && code_inj >= 0) {
+            // the tile column's one receiver (the table): its sample was loaded before the stencil
+            if (inj_j >= 0) {
+                const float a = fm(fm(fm(fm(fm(adjv, s_rk[i][k]), A.dt), A.dt), invdx), invdz);
+                setc(v, inj_j, fs_(comp(v, inj_j), a));
+            }
+        } else if (inject && z0 + 3 >= s_rz0[i] && z0 <= s_rz1[i] && code_inj == -2) {
+            // several receivers in the tile column: the column's list, in its order
             const ShotDesc &D = shots[cb + i];
             const int e0 = __ldg(D.colptr + x), e1 = __ldg(D.colptr + x + 1);
             const float *arow = D.adj_t + (long long)(it - 1) * D.ntr;
