@@ -9,11 +9,13 @@
 // mbarrier (the copies landed) and an "empty" one (every consumer warp is done with it);
 // consumer warps wait only on the stage they need, so they drift apart by up to NST
 // shots instead of meeting at a block-wide barrier per shot.  The six coefficient tiles
-// arrive once per block, by one more tensor copy, and stay in registers for all shots.
+// arrive once per block, by one more tensor copy, and stay in registers for all shots
+// (k_tile) or are read from shared memory per shot (k_tile3, three blocks per SM).
 // Out-of-range parts of a tile (grid edges) are zero-filled by the copy engine.
 //
-// Arithmetic uses the packed f32x2 add/sub/mul of sm_100 on pairs of neighbouring cells,
-// with every operation rounded separately in the reference's association order: the
+// Arithmetic uses the packed f32x2 add/sub/fma of sm_100 on pairs of neighbouring cells
+// (products of two fields as fma(a, b, -0), products by a stencil constant as scalar
+// multiplies), with every operation rounded separately in the reference's association order: the
 // results are bit-identical to the scalar __fadd_rn/__fmul_rn evaluation of
 // acoustic_iso2d_fd_it_6order (propagation.c:13-74) and to the reference's strict IEEE
 // build (MATH 0).  MATH 1 contracts multiply-adds into packed FMAs (within the FP32
@@ -24,7 +26,8 @@
 // mirror free surface (:76-101), pseudo-Hessian (:579-594), imaging (:700-714) and the
 // adjoint injection (:676-682).  Its branches are uniform over a tile wherever they can
 // be: only tiles that reach the free-surface rows, the source or the receiver rows take
-// the corresponding code.
+// the corresponding code.  Receivers are found through a per-block table of the chunk's
+// receivers in the tile (built once per block), both for sampling and for the injection.
 //
 // Every wait is bounded: a tile copy that has not landed after two seconds sets the
 // error word, the block waits (again bounded) for its copies in flight and returns.
