@@ -415,6 +415,8 @@ extern "C" int fwi_ctx_set_shots(fwi_ctx *c, const fwi_shot *shots, int nshot)
         if (s.ix_min < 0 || s.ix_max >= c->nx || nxx <= 0) return fail(FWI_ERR_ARG, "shot %d: bad window [%d,%d]", i, s.ix_min, s.ix_max);
         if (s.ntr <= 0 || s.ns <= 0 || s.sampleRate <= 0 || !s.src || !s.igx || !s.igz)
             return fail(FWI_ERR_ARG, "shot %d: ntr=%d ns=%d sampleRate=%d", i, s.ntr, s.ns, s.sampleRate);
+        // the step kernel's receiver tables encode a trace index in 23 bits
+        if (s.ntr >= (1 << 23)) return fail(FWI_ERR_ARG, "shot %d: %d receivers (at most %d)", i, s.ntr, (1 << 23) - 1);
         if ((c->nt - 1) / s.sampleRate + 1 > s.ns) return fail(FWI_ERR_ARG, "shot %d: ns=%d too short for nt=%d", i, s.ns, c->nt);
         if (!in_fd_range(s.isx, s.isz, c->nz, nxx, c->pml, c->fs))
             return fail(FWI_ERR_ARG, "shot %d: source (%d,%d) outside the updated grid", i, s.isx, s.isz);
