@@ -2294,6 +2294,7 @@ extern "C" int fwi_ctx_run(fwi_ctx *c, int problem, float freq, int filter, int 
         CK(cudaStreamSynchronize(c->stream));
         for (auto &k : keep) free_run(c, k.get());
     }
+    TRY(obs_join(c));  // a run that read no observed gathers still returns after their upload
     CK(cudaEventRecord(c->ev1, c->stream));
     CK(cudaEventSynchronize(c->ev1));
     TRY(check_kernel_error(c));

@@ -176,7 +176,10 @@ FWI_API int fwi_ctx_set_model(fwi_ctx *ctx, const float *vp, const float *rho, i
 FWI_API int fwi_ctx_set_model_device(fwi_ctx *ctx, const float *d_vp, const float *d_rho, int nz, int nx, float dx,
                              float dz, float dt, int nt, int pmlThick, int freesurface);
 FWI_API int fwi_ctx_set_shots(fwi_ctx *ctx, const fwi_shot *shots, int nshot);
-/* observed gathers: one host array [ntr][ns] per shot */
+/* observed gathers: one host array [ntr][ns] per shot.  The upload runs on a stream of its own,
+ * overlapping the next run's forward pass: page-locked arrays are read after the call returns, so
+ * keep them unchanged until the next fwi_ctx_run (or fwi_ctx_destroy) returns; pageable arrays
+ * are staged before the call returns. */
 FWI_API int fwi_ctx_set_observed(fwi_ctx *ctx, const float *const *obs);
 /* problem 0/1/2 as iso_acoustic2d_propagation; results stay on the device */
 FWI_API int fwi_ctx_run(fwi_ctx *ctx, int problem, float freq, int filter, int precondition, int path);
