@@ -378,13 +378,14 @@ __device__ __forceinline__ void tile_body(const CUtensorMap &tm_p1, const CUtens
     __shared__ int s_isx[TILE_CH_MAX], s_isz[TILE_CH_MAX], s_rz0[TILE_CH_MAX], s_rz1[TILE_CH_MAX];
     __shared__ bool s_spec[TILE_CH_MAX];
     __shared__ int s_fi[2];  // frames of p1 and p0 (the same for every shot of the chunk)
-    // TileSync mode: trace row of this step's sample per shot (or null), and the receivers of the
-    // chunk's shots in the tile's columns and rows, (trace << 8) | (row - first row of the tile),
-    // -1 none, -2 several (read from the receiver list)
+    // TileSync mode: trace row of this step's sample per shot (or null).  The receivers of the
+    // chunk's shots in the tile's columns and rows (for that sampling, and for the injection of
+    // every adjoint step): (trace << 8) | (row - first row of the tile), -1 none, -2 several
+    // (read from the receiver list)
     __shared__ float *s_tr[TILE_CH_MAX];
     __shared__ int s_rcv[TILE_CH_MAX][TX];
-    // adjoint steps: the same table for the injection, with each receiver's interpolation weight
-    // (recK) and the step's adjoint-source row per shot
+    // adjoint steps: each table entry's interpolation weight (recK), and the step's adjoint-source
+    // row per shot
     __shared__ float s_rk[TILE_CH_MAX][TX];
     __shared__ const float *s_adj[TILE_CH_MAX];
 
